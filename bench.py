@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark of the MSF hot path on the R-MAT scale-22 workload.
+
+Workload (one "step" = one full minimum-spanning-forest solve):
+  R-MAT scale 22 (4,194,304 vertices), edge factor 16 (2^26 draws, a, b, c, d =
+  .57, .19, .19, .05, no vertex permutation), self-loops dropped, duplicates
+  kept, uint32 weights uniform in [1, 2^20], edge ids in upper-triangle CSR
+  order; output = the unique MSF under (weight, edge id), its count and uint64
+  total.  Synthetic (seeded) input: the reference's benchmark files are not
+  available.
+
+  value   Gedges/s = input edges / device time per solve, edges resident in HBM
+          (805 MB, larger than L2, so no flush is needed between steps).
+  e2e     the same metric through the C ABI call phem_msf_solve with pinned HOST
+          edges in and host MSF records out (copies inside the timed region).
+  roofline  the dominant kernel's algorithmic bytes / its event-timed duration
+          against the measured HBM copy bandwidth.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl phem|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own shard of a
+global multigraph (same vertex set, seed 22 + rank, 2^26 draws each), the local
+forests are all-gathered over NCCL and every rank solves their union; value =
+all ranks' input edges / max-over-ranks time ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gedges/s + % HBM roofline for MST/CC; batched p50/p99 vs one-launch-per-solve"
+UNIT = "Gedges/s"
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed work runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [x for x in sm if x > 0.5 * (mx or 1)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def rmat22(rank: int = 0, scale: int = 22, edge_factor: int = 16):
+    from phem_graph_b200 import gen
+    g = gen.rmat_graph(scale, edge_factor, seed=22 + rank)
+    return g, g.msf_edges()
+
+
+def msf_algorithmic_bytes(m: int, n: int, m_r: list, n_r: list, count: int) -> dict:
+    """Algorithmic bytes.  'survey': the per-solve model
+    sum_r (32 m_r + 16 m_{r+1}) + 16 sum_r n_r + 12 (n - c).  Per kernel: the
+    records a kernel must read and write by its definition."""
+    survey = 0
+    for r, mr in enumerate(m_r):
+        nxt = m_r[r + 1] if r + 1 < len(m_r) else 0
+        survey += 32 * mr + 16 * nxt
+    survey += 16 * sum(n_r) + 12 * count
+    edge_pass = 0
+    for r in range(1, len(m_r) + 1):
+        rin = 12 * m if r == 1 else 16 * m_r[r - 1]
+        rout = 16 * (m_r[r] if r < len(m_r) else 0)
+        edge_pass += rin + rout
+    return {"survey": survey, "msf_edge_pass": edge_pass, "msf_round0": 12 * m,
+            "msf_hook": 36 * sum(n_r), "msf_gather": (m + 31) // 32 * 4 + 24 * count}
+
+
+def cpu_baseline_pbbs(E: np.ndarray, budget_s: float = 20.0, max_runs: int = 5) -> dict:
+    """The reference's PBBS mst() (oracle/_ref) on all host cores, call time only,
+    median of up to `max_runs` runs after one warm-up, bounded by `budget_s`."""
+    import oracle
+    if not oracle.ref_available():
+        flags, cnt, _ = None, None, None
+        t0 = time.perf_counter()
+        oracle.msf_kruskal(E, int(E[:, :2].max()) + 1)
+        dt = time.perf_counter() - t0
+        return {"value": len(E) / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": f"oracle Kruskal (w, id) on the full {len(E)}-edge array, 1 run"}
+    ref = oracle.RefPBBS(E)
+    times = []
+    t_start = time.perf_counter()
+    ref.run()  # warm-up
+    while len(times) < max_runs and time.perf_counter() - t_start < budget_s:
+        times.append(ref.run())
+    workers = ref.workers()
+    ref.close()
+    med = statistics.median(times)
+    return {"value": len(E) / med / 1e9, "unit": UNIT, "cores": workers, "kind": "reference",
+            "sample": f"PBBS mst() (MST/src/utils.cu) on the full {len(E)}-edge R-MAT-22 array, "
+                      f"median of {len(times)} runs after 1 warm-up, call time only",
+            "seconds_median": med}
+
+
+def run_reference(args) -> None:
+    """--impl reference: the reference's own CPU path (PBBS mst()) on the same
+    workload, all host threads; one step = one full solve."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    g, E = rmat22(0, args.scale, args.edge_factor)
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference tree absent)"}))
+        return
+    ref = oracle.RefPBBS(E)
+    for _ in range(args.warmup):
+        ref.run()
+    times = [ref.run() for _ in range(args.steps)]
+    workers = ref.workers()
+    total = sum(times)
+    value = args.steps * g.m / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"msf_rmat{args.scale}_ef{args.edge_factor}", "n": g.n, "m": g.m, "seed": 22,
+                   "weights": "uniform [1, 2^20]"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "reference",
+                         "sample": f"PBBS mst() on the full {g.m}-edge array, {args.steps} timed runs"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def profile_traffic(name: str):
+    """Per-launch DRAM traffic of a kernel from its committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"{name}.md"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("traffic_bytes_per_solve:"):
+            try:
+                return float(ln.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["phem", "reference"], default="phem")
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import phem_graph_b200 as P
+    from phem_graph_b200 import dist as pdist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    g, E = rmat22(rank, args.scale, args.edge_factor)
+    n, m = g.n, g.m
+    ctx = P.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream)
+    d_edges = torch.from_numpy(E.view(np.int32)).to(f"cuda:{local}")
+    d_out = torch.empty((n, 3), dtype=torch.int32, device=f"cuda:{local}")
+    d_ct = torch.zeros(2, dtype=torch.int64, device=f"cuda:{local}")
+    h_pinned = torch.from_numpy(E.view(np.int32)).pin_memory()
+    h_out = torch.empty((n, 3), dtype=torch.int32).pin_memory()
+
+    def step():
+        if world > 1:
+            return pdist.sharded_msf_device(ctx, d_edges, m, n, stream)
+        return ctx.msf_solve_device(d_edges, m, n, d_out, d_ct)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            res = step()
+    torch.cuda.synchronize()
+
+    peaks = measured_peaks()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.profile_reset()
+    ctx.set_profiling(True)
+    with ClockSampler(local) as clocks:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        with torch.cuda.stream(stream):
+            for _ in range(args.steps):
+                res = step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t_ms = ev0.elapsed_time(ev1)
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+
+        # end to end through the C ABI: pinned host edges in, host records out
+        e2e_steps = args.e2e_steps or max(3, min(args.steps, 10))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            r_host = ctx.msf_solve(h_pinned.numpy(), n)
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        tt = torch.tensor([t_ms, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms, e2e_s = float(tt[0]), float(tt[1])
+
+    ms_per_step = t_ms / args.steps
+    value = world * m / (ms_per_step / 1e3) / 1e9
+    gpu_launches = sum(v["launches"] for v in prof.values())
+
+    # roofline of the dominant kernel, event-timed inside the timed region
+    stats = ctx.msf_solve_device(d_edges, m, n, d_out, d_ct) if world > 1 else res
+    byts = msf_algorithmic_bytes(m, n, stats.m_r, stats.n_r, stats.count)
+    timed = {k: v for k, v in prof.items() if v["timed_launches"]}
+    dom = max(timed, key=lambda k: timed[k]["total_ms"]) if timed else None
+    kernels = {}
+    total_kernel_ms = sum(v["total_ms"] for v in timed.values()) or 1.0
+    for k, v in timed.items():
+        entry = {"launches": v["launches"], "ms_per_step": v["total_ms"] / args.steps,
+                 "share": v["total_ms"] / total_kernel_ms}
+        if k in byts:
+            gbs = byts[k] * args.steps / (v["total_ms"] / 1e3) / 1e9
+            entry.update({"bytes_per_step": byts[k], "achieved_gbs": gbs, "frac": gbs / peaks["hbm_gbs"]})
+        kernels[k] = entry
+    roofline = None
+    if dom:
+        achieved = kernels[dom].get("achieved_gbs")
+        traffic = profile_traffic(f"{dom}_rmat22")
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
+                    "traffic": traffic, "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes_per_step": byts.get(dom)}
+    solve_gbs = byts["survey"] / (ms_per_step / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"msf_rmat{args.scale}_ef{args.edge_factor}", "n": n, "m": m, "seed": 22,
+                   "weights": "uniform [1, 2^20]", "l2": "inputs larger than L2 (805 MB edge array), no flush",
+                   "parallelism": f"shard{world}" if world > 1 else "single"},
+        "roofline": roofline,
+        "solve_roofline": {"model": "sum_r(32 m_r + 16 m_r+1) + 16 sum_r n_r + 12 (n - c)",
+                           "bytes": byts["survey"], "achieved": solve_gbs, "peak": peaks["hbm_gbs"],
+                           "frac": solve_gbs / peaks["hbm_gbs"], "m_r": stats.m_r, "n_r": stats.n_r},
+        "kernels": kernels,
+        "result": {"msf_edges": stats.count, "total_weight": stats.total, "rounds": stats.rounds},
+        "e2e": {"value": world * m / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": m * 12,
+                "d2h_bytes_per_step": r_host.count * 12 + 16, "ms_per_step": e2e_s * 1e3,
+                "api": "phem_msf_solve (C ABI), pinned host edges"},
+        "gpu_launches": gpu_launches,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_pbbs(E)
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

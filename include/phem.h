@@ -1,0 +1,259 @@
+/*
+ * phem.h -- C ABI of the B200-native PHEM graph library (libphem.so).
+ *
+ * Two hot paths of the PHEM reference, rebuilt as sm_100a CUDA kernels:
+ *   - union-find connected components + spanning forest
+ *       (CC/ExternalSpanningTree.cu, CC/GPUSpanningTree.cu);
+ *   - Boruvka minimum spanning forest (MST/src/kernels.cu, MST/src/new_boruvka.cu).
+ *
+ * The reference exports name-mangled C++ functions that print and exit() on any
+ * CUDA error.  This header is the plain C boundary a foreign-function binding
+ * attaches to: POD arguments, pointers and sizes, status codes, no exit().
+ * Each entry point names the reference function it stands in for.
+ *
+ * Pointers.  Unless an entry point says "device", every array argument may be
+ * host memory (pageable or pinned) or device memory of the context's GPU; the
+ * library looks the pointer up and stages host arrays through its own device
+ * workspace, copying results back before it returns.  Device-resident inputs
+ * are never copied.
+ *
+ * Streams.  All GPU work of a context is ordered on its stream.  Entry points
+ * return after the work is complete unless they say "asynchronous".
+ *
+ * Errors.  A non-zero phem_status is returned; phem_last_error() gives a
+ * one-line description (thread-local).  Device loops are bounded: a loop that
+ * hits its cap sets a status word and the call returns PHEM_ERR_NONCONVERGED
+ * instead of hanging.
+ */
+#ifndef PHEM_H
+#define PHEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHEM_VERSION 100
+
+typedef enum phem_status {
+    PHEM_OK = 0,
+    PHEM_ERR_INVALID = 1,        /* bad argument: size, range, null pointer, endpoint >= n */
+    PHEM_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    PHEM_ERR_NOMEM = 3,          /* device or pinned allocation failed */
+    PHEM_ERR_NONCONVERGED = 4,   /* a bounded device loop reached its cap */
+    PHEM_ERR_TIMEOUT = 5,        /* the host watchdog deadline passed */
+    PHEM_ERR_UNSUPPORTED = 6,    /* valid request outside what this build supports */
+    PHEM_ERR_NO_DEVICE = 7       /* no CUDA device, or the device is not sm_100 */
+} phem_status;
+
+/* MSF edge record, MST/src/constants.h:15-19 (`edge`: vertex u, vertex v, weight w;
+ * all uint32).  Records are 12 bytes, array of structures. */
+typedef struct phem_edge {
+    uint32_t u;
+    uint32_t v;
+    uint32_t w;
+} phem_edge;
+
+/* Empty forest slot, INT_MAX held in a uint64 (CC/ExternalSpanningTree.cu:114,
+ * CC/GPUSpanningTree.cu:139). */
+#define PHEM_FOREST_EMPTY 0x7fffffffULL
+
+/* Upper bound on Boruvka rounds (each round at least halves the live
+ * components, so 33 suffice for 2^32 vertices); the reference caps at 100
+ * (MST/src/kernels.cu:679-682). */
+#define PHEM_MAX_ROUNDS 64
+
+typedef struct phem_context phem_context;
+
+/* ---------------------------------------------------------------- context */
+
+/* Binds a context to CUDA device `device` and creates its stream.  Fails with
+ * PHEM_ERR_NO_DEVICE when the device is missing or is not compute capability
+ * 10.x (the kernels are built for sm_100a only). */
+phem_status phem_context_create(int device, phem_context **out);
+void phem_context_destroy(phem_context *ctx);
+
+/* Orders the context's work on `stream` (a cudaStream_t of the same device);
+ * NULL restores the context's own stream. */
+phem_status phem_context_set_stream(phem_context *ctx, void *stream);
+void *phem_context_stream(phem_context *ctx);
+
+/* Host watchdog for the synchronous entry points: when a solve has not
+ * finished `ms` milliseconds after it was queued the call returns
+ * PHEM_ERR_TIMEOUT (the work itself is left to finish; the device is never
+ * reset).  0 disables the watchdog (default). */
+phem_status phem_context_set_timeout_ms(phem_context *ctx, uint32_t ms);
+
+/* Per-kernel accounting.  Every kernel launch is counted; with profiling on,
+ * each launch is also bracketed by CUDA events on the context stream and its
+ * duration added up (for roofline figures measured inside an application). */
+typedef struct phem_kernel_profile {
+    char name[32];
+    uint64_t launches;        /* launches since the last reset */
+    uint64_t timed_launches;  /* launches that were event-timed */
+    double total_ms;          /* summed event time of the timed launches */
+} phem_kernel_profile;
+
+phem_status phem_context_set_profiling(phem_context *ctx, int on);
+/* Copies up to `max` entries (kernels launched at least once) and sets *count
+ * to the number available.  Synchronises the context stream. */
+phem_status phem_context_profile(phem_context *ctx, phem_kernel_profile *out, uint32_t max, uint32_t *count);
+phem_status phem_context_profile_reset(phem_context *ctx);
+
+/* Releases the context's device workspace (it grows on demand otherwise). */
+phem_status phem_context_trim(phem_context *ctx);
+
+const char *phem_status_string(phem_status s);
+const char *phem_last_error(void);
+int phem_version(void);
+
+/* ---------------------------------------------------------------- statistics */
+
+typedef struct phem_cc_stats {
+    uint64_t forest_edges;  /* edges written to the forest (= n - components) */
+    uint32_t components;    /* number of distinct labels */
+    uint32_t rounds;        /* Boruvka rounds (canonical forest only, else 0) */
+    float device_ms;        /* GPU time of the solve, CUDA events on the stream */
+} phem_cc_stats;
+
+typedef struct phem_msf_stats {
+    uint32_t rounds;                     /* rounds that hooked at least one component */
+    uint32_t pad;
+    uint64_t m_r[PHEM_MAX_ROUNDS];       /* live edges entering round r */
+    uint64_t n_r[PHEM_MAX_ROUNDS];       /* components with a live edge entering round r */
+    uint64_t msf_edges;                  /* = n - components */
+    uint64_t total_weight;               /* uint64 sum of MSF weights */
+    float device_ms;                     /* GPU time of the solve, CUDA events on the stream */
+} phem_msf_stats;
+
+/* -------------------------------------------------- connected components / SF */
+
+/* Forest selection for phem_cc_solve. */
+#define PHEM_CC_DEFAULT 0u
+/* The forest is the minimum spanning forest under edge index order: the edge
+ * SET that the reference's CPU path (CC/host_spanning_tree.cu:67-86) produces
+ * with one Parlay worker.  Without the flag the forest is whichever edges won
+ * the hooking races, as in the reference GPU kernels. */
+#define PHEM_CC_CANONICAL 1u
+
+/* One-shot CC + spanning forest over packed edges (u << 32 | v).
+ * Replaces init_parent_label_T1edges + union_find_gpu_COO + cc
+ * (CC/ExternalSpanningTree.cu:77-116, CC/GPUSpanningTree.cu:122-128).
+ *   labels[n]  <- smallest vertex id of each vertex's component;
+ *   forest[n]  <- at slot r, the edge whose union hooked root r; other slots
+ *                 PHEM_FOREST_EMPTY (forest may be NULL).
+ * Edges with u >= v are skipped, as union_find_gpu_COO skips them
+ * (CC/ExternalSpanningTree.cu:82).  Endpoints must be < n (else INVALID).
+ * PHEM_CC_CANONICAL requires m < 2^32.  stats may be NULL. */
+phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, int32_t n,
+                          int32_t *labels, uint64_t *forest, uint32_t flags, phem_cc_stats *stats);
+
+/* Stage-level entry points on DEVICE arrays, asynchronous on the context stream. */
+
+/* parent[i] = label[i] = i, forest[i] = PHEM_FOREST_EMPTY.
+ * init_parent_label_T1edges / _T2edges (CC/ExternalSpanningTree.cu:108-116,
+ * CC/GPUSpanningTree.cu:132-140).  label or forest may be NULL. */
+phem_status phem_cc_init(phem_context *ctx, int32_t n, int32_t *d_parent, int32_t *d_label,
+                         uint64_t *d_forest);
+
+/* Unions a batch of packed edges into the resident parent array and records
+ * hooks in forest.  union_find_gpu_COO / COO1 (CC/ExternalSpanningTree.cu:77-97). */
+phem_status phem_cc_unite(phem_context *ctx, const uint64_t *d_edges, int64_t m, int32_t n,
+                          int32_t *d_parent, uint64_t *d_forest);
+
+/* label[i] = find(i) with path compression.  cc (CC/GPUSpanningTree.cu:122-128). */
+phem_status phem_cc_label(phem_context *ctx, int32_t n, int32_t *d_parent, int32_t *d_label);
+
+/* Streaming spanning forest over host-resident batches.
+ * SpanningTree (CC/ExternalSpanningTree.cu:133-218): initialises the state,
+ * streams h_edges[0..m) to the GPU in batches of `batch` edges through
+ * double-buffered copies overlapped with the union kernels, and leaves the
+ * union-find state in d_parent and the per-batch forest in d_forest (both n
+ * entries, device).  d_label is initialised to the identity.  h_edges should
+ * be pinned for the copies to overlap.  *ms receives the event time. */
+phem_status phem_cc_stream(phem_context *ctx, const uint64_t *h_edges, int64_t m, int32_t n,
+                           int64_t batch, int32_t *d_parent, int32_t *d_label, uint64_t *d_forest,
+                           float *ms);
+
+/* Merge of two forests into final labels and a final forest.
+ * gpu_spanning_tree (CC/GPUSpanningTree.cu:169-198): resets the state, unions
+ * the 2n candidates d_forest_a[n] ++ d_forest_b[n] (PHEM_FOREST_EMPTY slots and
+ * u >= v skipped), writes d_forest_out[n] and d_label[n] (min id).  d_forest_b
+ * may be NULL (n empty slots).  *ms receives the event time. */
+phem_status phem_cc_merge(phem_context *ctx, const uint64_t *d_forest_a, const uint64_t *d_forest_b,
+                          int32_t n, int32_t *d_parent, int32_t *d_label, uint64_t *d_forest_out,
+                          float *ms);
+
+/* ------------------------------------------------------------ minimum spanning forest */
+
+/* Minimum spanning forest of edges[0..m) over vertices [0, n) under the strict
+ * order (w, edge index).  Stands in for boruvka_for_edge_array
+ * (MST/src/new_boruvka.cu:40-179) and the PBBS mst() (MST/src/utils.cu:794-841):
+ *   msf[0..*count) <- the MSF edges, ascending by edge index (the order of the
+ *                     PBBS result, utils.cu:837,871-885); msf needs room for
+ *                     n - 1 records and may be NULL;
+ *   *count, *total <- number of MSF edges and their uint64 total weight.
+ * Self-loops are ignored.  Endpoints must be < n.  m < 2^32.  count, total and
+ * stats may be NULL. */
+phem_status phem_msf_solve(phem_context *ctx, const phem_edge *edges, uint64_t m, uint32_t n,
+                           phem_edge *msf, uint64_t *count, uint64_t *total, phem_msf_stats *stats);
+
+/* Same on DEVICE arrays: d_msf (room for n - 1 records, may be NULL) gets the
+ * records and d_count_total[0], d_count_total[1] the count and total weight
+ * (may be NULL).  Stands in for device_boruvka (MST/src/kernels.cu:507-689),
+ * which works on caller-owned device buffers.  Returns when the solve is done. */
+phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, uint64_t m, uint32_t n,
+                                  phem_edge *d_msf, uint64_t *d_count_total, phem_msf_stats *stats);
+
+/* MSF of a symmetrised CSR graph (int64 offsets[n + 1], uint32 cols[2m]).
+ * Edge i is the i-th entry with row < col in row-major order (the numbering of
+ * csr_to_coo, CC/graph.cu:169-187); weights[i] is its weight.  Output as
+ * phem_msf_solve. */
+phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const uint32_t *cols,
+                               uint32_t n, const uint32_t *weights, uint64_t m_upper,
+                               phem_edge *msf, uint64_t *count, uint64_t *total,
+                               phem_msf_stats *stats);
+
+/* CSR -> packed COO (row << 32 | col) for entries with row < col, in row-major
+ * order.  csr_to_coo (CC/graph.cu:149-196), on the GPU.  out needs room for
+ * the number of such entries (NULL to count only); *out_m receives it. */
+phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, int32_t n,
+                            uint64_t *out, int64_t *out_m);
+
+/* --------------------------------------------------------- synthetic inputs (host) */
+/* Seeded generators for tests and benchmarks (no reference counterpart: the
+ * reference reads graph files).  Deterministic for any thread count. */
+
+/* SplitMix64 value i of stream `tag` under `seed`. */
+uint64_t phem_gen_mix64(uint64_t seed, uint64_t tag, uint64_t i);
+
+/* Erdos-Renyi: `draws` uniform pairs over [0, n); self-loops dropped,
+ * duplicates kept, packed (min << 32 | max) in draw order.  out needs `draws`
+ * entries (NULL to count); *out_m receives the number kept. */
+phem_status phem_gen_er(uint32_t n, uint64_t draws, uint64_t seed, uint64_t *out, uint64_t *out_m);
+
+/* R-MAT (Chakrabarti, Zhan, Faloutsos 2004) on 2^scale vertices with quadrant
+ * probabilities a, b, c (d = 1 - a - b - c), no vertex permutation; self-loops
+ * dropped, duplicates kept; pairs packed (min << 32 | max) and sorted, i.e. the
+ * upper triangle of the symmetrised CSR in row-major order.  out needs `draws`
+ * entries (NULL to count). */
+phem_status phem_gen_rmat(uint32_t scale, uint64_t draws, double a, double b, double c, uint64_t seed,
+                          uint64_t *out, uint64_t *out_m);
+
+/* w[i] = 1 + (SplitMix64 value i & (2^bits - 1)), i.e. uniform in [1, 2^bits]. */
+phem_status phem_gen_weights(uint64_t m, uint64_t seed, uint32_t bits, uint32_t *w);
+
+/* {u, v, w} records from packed pairs and weights (w may be NULL: zero). */
+phem_status phem_pack_msf_edges(const uint64_t *pairs, const uint32_t *w, uint64_t m, phem_edge *out);
+
+/* Symmetrised CSR from pairs sorted by (u, v) with u < v. */
+phem_status phem_csr_from_sorted_pairs(const uint64_t *pairs, uint64_t m, uint32_t n, int64_t *offsets,
+                                       uint32_t *cols);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHEM_H */

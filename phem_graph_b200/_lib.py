@@ -1,0 +1,132 @@
+"""ctypes binding of libphem.so (include/phem.h).
+
+The library is the product: if it is missing this module raises instead of
+falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libphem.so"
+
+PHEM_OK = 0
+PHEM_ERR_INVALID = 1
+PHEM_ERR_CUDA = 2
+PHEM_ERR_NOMEM = 3
+PHEM_ERR_NONCONVERGED = 4
+PHEM_ERR_TIMEOUT = 5
+PHEM_ERR_UNSUPPORTED = 6
+PHEM_ERR_NO_DEVICE = 7
+PHEM_FOREST_EMPTY = 0x7FFFFFFF
+PHEM_MAX_ROUNDS = 64
+PHEM_CC_DEFAULT = 0
+PHEM_CC_CANONICAL = 1
+
+
+class PhemError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        super().__init__(f"{where}: status {status}: {detail}")
+        self.status = status
+
+
+class PhemEdge(C.Structure):
+    _fields_ = [("u", C.c_uint32), ("v", C.c_uint32), ("w", C.c_uint32)]
+
+
+class CCStats(C.Structure):
+    _fields_ = [("forest_edges", C.c_uint64), ("components", C.c_uint32), ("rounds", C.c_uint32),
+                ("device_ms", C.c_float)]
+
+
+class MSFStats(C.Structure):
+    _fields_ = [("rounds", C.c_uint32), ("pad", C.c_uint32),
+                ("m_r", C.c_uint64 * PHEM_MAX_ROUNDS), ("n_r", C.c_uint64 * PHEM_MAX_ROUNDS),
+                ("msf_edges", C.c_uint64), ("total_weight", C.c_uint64), ("device_ms", C.c_float)]
+
+
+class KernelProfile(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint64), ("timed_launches", C.c_uint64),
+                ("total_ms", C.c_double)]
+
+
+_VP = C.c_void_p
+_lib = None
+
+# name -> (restype, argtypes); mirrors include/phem.h
+SIGNATURES = {
+    "phem_version": (C.c_int, []),
+    "phem_status_string": (C.c_char_p, [C.c_int]),
+    "phem_last_error": (C.c_char_p, []),
+    "phem_context_create": (C.c_int, [C.c_int, C.POINTER(_VP)]),
+    "phem_context_destroy": (None, [_VP]),
+    "phem_context_set_stream": (C.c_int, [_VP, _VP]),
+    "phem_context_stream": (_VP, [_VP]),
+    "phem_context_set_timeout_ms": (C.c_int, [_VP, C.c_uint32]),
+    "phem_context_trim": (C.c_int, [_VP]),
+    "phem_context_set_profiling": (C.c_int, [_VP, C.c_int]),
+    "phem_context_profile": (C.c_int, [_VP, C.POINTER(KernelProfile), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "phem_context_profile_reset": (C.c_int, [_VP]),
+    "phem_cc_solve": (C.c_int, [_VP, _VP, C.c_int64, C.c_int32, _VP, _VP, C.c_uint32, C.POINTER(CCStats)]),
+    "phem_cc_init": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
+    "phem_cc_unite": (C.c_int, [_VP, _VP, C.c_int64, C.c_int32, _VP, _VP]),
+    "phem_cc_label": (C.c_int, [_VP, C.c_int32, _VP, _VP]),
+    "phem_cc_stream": (C.c_int, [_VP, _VP, C.c_int64, C.c_int32, C.c_int64, _VP, _VP, _VP,
+                                 C.POINTER(C.c_float)]),
+    "phem_cc_merge": (C.c_int, [_VP, _VP, _VP, C.c_int32, _VP, _VP, _VP, C.POINTER(C.c_float)]),
+    "phem_msf_solve": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, _VP, C.POINTER(C.c_uint64),
+                                 C.POINTER(C.c_uint64), C.POINTER(MSFStats)]),
+    "phem_msf_solve_device": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, _VP, _VP, C.POINTER(MSFStats)]),
+    "phem_msf_solve_csr": (C.c_int, [_VP, _VP, _VP, C.c_uint32, _VP, C.c_uint64, _VP, C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_uint64), C.POINTER(MSFStats)]),
+    "phem_csr_to_coo": (C.c_int, [_VP, _VP, _VP, C.c_int32, _VP, C.POINTER(C.c_int64)]),
+    "phem_gen_mix64": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
+    "phem_gen_er": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint64, _VP, C.POINTER(C.c_uint64)]),
+    "phem_gen_rmat": (C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64, _VP,
+                                C.POINTER(C.c_uint64)]),
+    "phem_gen_weights": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, _VP]),
+    "phem_pack_msf_edges": (C.c_int, [_VP, _VP, C.c_uint64, _VP]),
+    "phem_csr_from_sorted_pairs": (C.c_int, [_VP, C.c_uint64, C.c_uint32, _VP, _VP]),
+}
+
+
+def lib() -> C.CDLL:
+    """The loaded libphem.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m phem_graph_b200.build` "
+                              "(there is no fallback implementation)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != PHEM_OK:
+        detail = lib().phem_last_error()
+        raise PhemError(status, where, detail.decode() if detail else "")
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array, a torch tensor or an int; None for None."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"cannot take the address of {type(a)!r}")

@@ -1,0 +1,196 @@
+"""Python view of the C ABI: a Context bound to one GPU and its solves.
+
+Arrays may be numpy (host) or torch CUDA tensors (device); the library stages
+host arrays itself.  Results come back as numpy arrays unless device outputs
+are passed in.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import (CCStats, KernelProfile, MSFStats, PHEM_CC_CANONICAL, PHEM_FOREST_EMPTY, check, lib, ptr)
+
+# phem_edge as a numpy structured dtype (MST/src/constants.h:15-19)
+EDGE_DTYPE = np.dtype([("u", "<u4"), ("v", "<u4"), ("w", "<u4")])
+
+
+def as_edges(E) -> np.ndarray:
+    """{u, v, w} records as an (m, 3) uint32 C array."""
+    if isinstance(E, np.ndarray) and E.dtype == EDGE_DTYPE:
+        return E.view(np.uint32).reshape(-1, 3)
+    E = np.ascontiguousarray(E, np.uint32)
+    return E.reshape(-1, 3)
+
+
+@dataclass
+class CCResult:
+    labels: np.ndarray
+    forest: np.ndarray | None
+    components: int
+    forest_edges: int
+    rounds: int
+    device_ms: float
+
+
+@dataclass
+class MSFResult:
+    edges: np.ndarray          # (count, 3) uint32, ascending by edge id
+    count: int
+    total: int
+    rounds: int
+    m_r: list = field(default_factory=list)
+    n_r: list = field(default_factory=list)
+    device_ms: float = 0.0
+
+
+class Context:
+    """A libphem context on CUDA device `device` (its own stream and workspace)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        check(lib().phem_context_create(device, C.byref(self._h)), "phem_context_create")
+        self.device = device
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def close(self) -> None:
+        if self._h:
+            lib().phem_context_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream) -> None:
+        """Orders work on a CUDA stream (torch.cuda.Stream, raw handle, or None)."""
+        h = getattr(stream, "cuda_stream", stream)
+        check(lib().phem_context_set_stream(self._h, h), "phem_context_set_stream")
+
+    def set_timeout_ms(self, ms: int) -> None:
+        check(lib().phem_context_set_timeout_ms(self._h, ms), "phem_context_set_timeout_ms")
+
+    def trim(self) -> None:
+        check(lib().phem_context_trim(self._h), "phem_context_trim")
+
+    def set_profiling(self, on: bool) -> None:
+        """Brackets every kernel launch with CUDA events (per-kernel durations)."""
+        check(lib().phem_context_set_profiling(self._h, 1 if on else 0), "phem_context_set_profiling")
+
+    def profile(self) -> dict:
+        """{kernel name: {"launches", "timed_launches", "total_ms"}} since the last reset."""
+        buf = (KernelProfile * 64)()
+        cnt = C.c_uint32()
+        check(lib().phem_context_profile(self._h, buf, 64, C.byref(cnt)), "phem_context_profile")
+        return {buf[i].name.decode(): {"launches": int(buf[i].launches), "timed_launches": int(buf[i].timed_launches),
+                                       "total_ms": float(buf[i].total_ms)} for i in range(min(cnt.value, 64))}
+
+    def profile_reset(self) -> None:
+        check(lib().phem_context_profile_reset(self._h), "phem_context_profile_reset")
+
+    def launches(self) -> int:
+        return sum(v["launches"] for v in self.profile().values())
+
+    # ------------------------------------------------------------ CC
+    def cc_solve(self, edges, n: int, canonical: bool = False, labels=None, forest=None,
+                 want_forest: bool = True) -> CCResult:
+        """Labels (min vertex id per component) and forest slots of packed
+        edges (u << 32 | v); see phem_cc_solve."""
+        m = int(edges.numel() if hasattr(edges, "numel") else len(edges))
+        if isinstance(edges, np.ndarray):
+            edges = np.ascontiguousarray(edges, np.uint64)
+        out_l = labels if labels is not None else np.empty(n, np.int32)
+        out_f = forest if forest is not None else (np.empty(n, np.uint64) if want_forest else None)
+        st = CCStats()
+        check(lib().phem_cc_solve(self._h, ptr(edges), m, n, ptr(out_l), ptr(out_f),
+                                  PHEM_CC_CANONICAL if canonical else 0, C.byref(st)), "phem_cc_solve")
+        return CCResult(out_l, out_f, int(st.components), int(st.forest_edges), int(st.rounds),
+                        float(st.device_ms))
+
+    def cc_init(self, n, parent, label=None, forest=None):
+        check(lib().phem_cc_init(self._h, n, ptr(parent), ptr(label), ptr(forest)), "phem_cc_init")
+
+    def cc_unite(self, edges, m, n, parent, forest=None):
+        check(lib().phem_cc_unite(self._h, ptr(edges), m, n, ptr(parent), ptr(forest)), "phem_cc_unite")
+
+    def cc_label(self, n, parent, label):
+        check(lib().phem_cc_label(self._h, n, ptr(parent), ptr(label)), "phem_cc_label")
+
+    def cc_stream(self, h_edges, n: int, batch: int, parent, label, forest) -> float:
+        """SpanningTree: host-resident batches through overlapped copies."""
+        ms = C.c_float()
+        m = len(h_edges) if isinstance(h_edges, np.ndarray) else int(h_edges.numel())
+        check(lib().phem_cc_stream(self._h, ptr(h_edges), m, n, batch, ptr(parent), ptr(label), ptr(forest),
+                                   C.byref(ms)), "phem_cc_stream")
+        return ms.value
+
+    def cc_merge(self, forest_a, forest_b, n: int, parent, label, forest_out) -> float:
+        """gpu_spanning_tree: merge two forests into final labels + forest."""
+        ms = C.c_float()
+        check(lib().phem_cc_merge(self._h, ptr(forest_a), ptr(forest_b), n, ptr(parent), ptr(label),
+                                  ptr(forest_out), C.byref(ms)), "phem_cc_merge")
+        return ms.value
+
+    # ------------------------------------------------------------ MSF
+    def msf_solve(self, edges, n: int, want_edges: bool = True) -> MSFResult:
+        """Unique MSF under (w, id) of {u, v, w} records; see phem_msf_solve."""
+        if isinstance(edges, np.ndarray):
+            edges = as_edges(edges)
+            m = len(edges)
+        else:  # torch tensor of shape (m, 3) uint32/int32 on the device
+            m = int(edges.shape[0])
+        out = np.empty((max(n - 1, 1), 3), np.uint32) if want_edges else None
+        cnt, tot = C.c_uint64(), C.c_uint64()
+        st = MSFStats()
+        check(lib().phem_msf_solve(self._h, ptr(edges), m, n, ptr(out), C.byref(cnt), C.byref(tot), C.byref(st)),
+              "phem_msf_solve")
+        k = int(cnt.value)
+        r = int(st.rounds)
+        return MSFResult(out[:k] if out is not None else None, k, int(tot.value), r,
+                         [int(x) for x in st.m_r[:r]], [int(x) for x in st.n_r[:r]], float(st.device_ms))
+
+    def msf_solve_device(self, d_edges, m: int, n: int, d_msf=None, d_count_total=None) -> MSFResult:
+        """Device-resident solve (torch tensors); counts stay on the device
+        unless d_count_total is given."""
+        st = MSFStats()
+        check(lib().phem_msf_solve_device(self._h, ptr(d_edges), m, n, ptr(d_msf), ptr(d_count_total),
+                                          C.byref(st)), "phem_msf_solve_device")
+        r = int(st.rounds)
+        return MSFResult(None, int(st.msf_edges), int(st.total_weight), r, [int(x) for x in st.m_r[:r]],
+                         [int(x) for x in st.n_r[:r]], float(st.device_ms))
+
+    def msf_solve_csr(self, offsets, cols, n: int, weights, m_upper: int) -> MSFResult:
+        out = np.empty((max(n - 1, 1), 3), np.uint32)
+        cnt, tot = C.c_uint64(), C.c_uint64()
+        st = MSFStats()
+        check(lib().phem_msf_solve_csr(self._h, ptr(offsets), ptr(cols), n, ptr(weights), m_upper, ptr(out),
+                                       C.byref(cnt), C.byref(tot), C.byref(st)), "phem_msf_solve_csr")
+        k = int(cnt.value)
+        r = int(st.rounds)
+        return MSFResult(out[:k], k, int(tot.value), r, [int(x) for x in st.m_r[:r]],
+                         [int(x) for x in st.n_r[:r]], float(st.device_ms))
+
+    def csr_to_coo(self, offsets, cols, n: int) -> np.ndarray:
+        nnz = int(offsets[n])
+        out = np.empty(max(nnz, 1), np.uint64)
+        k = C.c_int64()
+        check(lib().phem_csr_to_coo(self._h, ptr(offsets), ptr(cols), n, ptr(out), C.byref(k)), "phem_csr_to_coo")
+        return out[: k.value]
+
+
+def forest_set(forest: np.ndarray) -> np.ndarray:
+    f = np.asarray(forest, np.uint64)
+    return np.sort(f[f != np.uint64(PHEM_FOREST_EMPTY)])

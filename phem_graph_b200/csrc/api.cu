@@ -1,0 +1,848 @@
+// api.cu -- the C ABI of libphem.so (include/phem.h).
+//
+// Host orchestration only: argument checks, the context (stream, grow-only
+// workspace, control block), staging of host arrays through the workspace,
+// and the mapping of device status bits to phem_status.  No graph arithmetic
+// happens here and there is no CPU path: without a usable sm_100 device every
+// solve fails with PHEM_ERR_NO_DEVICE.
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+#include "internal.h"
+
+namespace phem {
+
+namespace {
+thread_local char g_last_error[512] = "";
+
+// Makes ctx->device current for the duration of a call, restoring the caller's.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+            prev = -1;
+        if (prev != dev)
+            ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev)
+            cudaSetDevice(prev);
+    }
+};
+
+// A caller array staged through the workspace when it is host memory.
+struct Staged {
+    void *dev = nullptr;   // pointer the kernels use
+    void *host = nullptr;  // caller's host pointer (null when it was already device memory)
+    size_t bytes = 0;
+};
+
+phem_status check_ctx(phem_context *ctx)
+{
+    if (!ctx) {
+        set_error("null context");
+        return PHEM_ERR_INVALID;
+    }
+    return PHEM_OK;
+}
+
+// Event-timed region on the context stream.
+struct Timed {
+    phem_context *ctx;
+    explicit Timed(phem_context *c) : ctx(c) { cudaEventRecord(ctx->ev_start, ctx->stream); }
+    float stop()
+    {
+        float ms = 0.f;
+        cudaEventRecord(ctx->ev_stop, ctx->stream);
+        if (cudaEventSynchronize(ctx->ev_stop) == cudaSuccess)
+            cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+        return ms;
+    }
+};
+
+}  // namespace
+
+const char *const kKernelNames[kKernelCount] = {
+    "msf_init", "msf_round0", "msf_edge_pass", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
+    "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "csr_pack"};
+
+static cudaEvent_t pool_get(phem_context *ctx)
+{
+    if (!ctx->event_pool.empty()) {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+
+KernelScope::KernelScope(phem_context *c, int k) : ctx(c), kernel(k)
+{
+    ctx->launches[k]++;
+    if (ctx->profiling) {
+        start = pool_get(ctx);
+        if (start)
+            cudaEventRecord(start, ctx->stream);
+    }
+}
+
+KernelScope::~KernelScope()
+{
+    if (!start)
+        return;
+    cudaEvent_t stop = pool_get(ctx);
+    if (!stop) {
+        ctx->event_pool.push_back(start);
+        return;
+    }
+    cudaEventRecord(stop, ctx->stream);
+    ctx->pending.push_back({kernel, start, stop});
+}
+
+void resolve_timings(phem_context *ctx)
+{
+    for (auto &p : ctx->pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.stop) == cudaSuccess && cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+            ctx->kernel_ms[p.kernel] += ms;
+            ctx->timed_launches[p.kernel]++;
+        }
+        ctx->event_pool.push_back(p.start);
+        ctx->event_pool.push_back(p.stop);
+    }
+    ctx->pending.clear();
+}
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+}
+
+bool is_device_ptr(const void *p)
+{
+    if (!p)
+        return false;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();  // clear the sticky-free error from an unknown pointer
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+uint64_t next_epochs(phem_context *ctx, uint32_t count)
+{
+    // Epochs are stored in 30 bits of a status word.  Before they wrap the
+    // status array is cleared so that no word from an old launch can match.
+    if (((ctx->epoch + count) >> 30) != (ctx->epoch >> 30) || ctx->epoch + count >= (1ull << 30)) {
+        if (ctx->status && ctx->status_words)
+            cudaMemsetAsync(ctx->status, 0, ctx->status_words * sizeof(uint64_t), ctx->stream);
+        ctx->epoch = 1;
+    }
+    const uint64_t e = ctx->epoch;
+    ctx->epoch += count;
+    return e;
+}
+
+phem_status ws_reserve(phem_context *ctx, size_t bytes)
+{
+    if (bytes <= ctx->ws_bytes)
+        return PHEM_OK;
+    PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->ws) {
+        cudaFree(ctx->ws);
+        ctx->ws = nullptr;
+        ctx->ws_bytes = 0;
+    }
+    const size_t want = bytes + bytes / 8;  // some headroom against small growth steps
+    if (cudaMalloc(&ctx->ws, want) != cudaSuccess) {
+        cudaGetLastError();
+        if (cudaMalloc(&ctx->ws, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->ws = nullptr;
+            set_error("workspace: cannot allocate %zu bytes", bytes);
+            return PHEM_ERR_NOMEM;
+        }
+        ctx->ws_bytes = bytes;
+        return PHEM_OK;
+    }
+    ctx->ws_bytes = want;
+    return PHEM_OK;
+}
+
+phem_status status_reserve(phem_context *ctx, size_t words)
+{
+    if (words <= ctx->status_words)
+        return PHEM_OK;
+    PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->status)
+        cudaFree(ctx->status);
+    ctx->status = nullptr;
+    ctx->status_words = 0;
+    const size_t want = words + words / 8 + 64;
+    if (cudaMalloc(&ctx->status, want * sizeof(uint64_t)) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->status = nullptr;
+        set_error("look-back status: cannot allocate %zu words", want);
+        return PHEM_ERR_NOMEM;
+    }
+    PHEM_CUDA_TRY(cudaMemsetAsync(ctx->status, 0, want * sizeof(uint64_t), ctx->stream));
+    ctx->status_words = want;
+    return PHEM_OK;
+}
+
+phem_status stream_wait(phem_context *ctx)
+{
+    if (!ctx->timeout_ms) {
+        PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        resolve_timings(ctx);
+        return PHEM_OK;
+    }
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(ctx->timeout_ms);
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) {
+            resolve_timings(ctx);
+            return PHEM_OK;
+        }
+        if (e != cudaErrorNotReady) {
+            set_error("stream: %s", cudaGetErrorString(e));
+            return PHEM_ERR_CUDA;
+        }
+        if (std::chrono::steady_clock::now() > deadline) {
+            set_error("watchdog: work not finished after %u ms", ctx->timeout_ms);
+            return PHEM_ERR_TIMEOUT;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+phem_status ctl_status(uint32_t err, const char *what)
+{
+    if (!err)
+        return PHEM_OK;
+    if (err & kErrRange) {
+        set_error("%s: an edge endpoint is >= n", what);
+        return PHEM_ERR_INVALID;
+    }
+    set_error("%s: device loop bound reached (status bits 0x%x)", what, err);
+    return PHEM_ERR_NONCONVERGED;
+}
+
+namespace {
+
+// Stages `bytes` of a caller input into the workspace at `off` when it is host
+// memory (queued on the context stream).
+phem_status stage_in(phem_context *ctx, const void *p, size_t bytes, size_t off, Staged *st)
+{
+    st->bytes = bytes;
+    if (is_device_ptr(p)) {
+        st->dev = const_cast<void *>(p);
+        st->host = nullptr;
+        return PHEM_OK;
+    }
+    st->dev = static_cast<char *>(ctx->ws) + off;
+    st->host = nullptr;
+    if (bytes)
+        PHEM_CUDA_TRY(cudaMemcpyAsync(st->dev, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return PHEM_OK;
+}
+
+// An output: device pointer used directly, host pointer via workspace at `off`.
+void stage_out(phem_context *ctx, void *p, size_t bytes, size_t off, Staged *st)
+{
+    st->bytes = bytes;
+    if (!p || is_device_ptr(p)) {
+        st->dev = p;
+        st->host = nullptr;
+        return;
+    }
+    st->dev = static_cast<char *>(ctx->ws) + off;
+    st->host = p;
+}
+
+phem_status copy_back(phem_context *ctx, const Staged &st, size_t bytes)
+{
+    if (st.host && bytes)
+        PHEM_CUDA_TRY(cudaMemcpyAsync(st.host, st.dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return PHEM_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace phem
+
+using namespace phem;
+
+extern "C" {
+
+int phem_version(void) { return PHEM_VERSION; }
+
+const char *phem_last_error(void) { return g_last_error; }
+
+const char *phem_status_string(phem_status s)
+{
+    switch (s) {
+    case PHEM_OK: return "ok";
+    case PHEM_ERR_INVALID: return "invalid argument";
+    case PHEM_ERR_CUDA: return "CUDA error";
+    case PHEM_ERR_NOMEM: return "out of memory";
+    case PHEM_ERR_NONCONVERGED: return "device loop bound reached";
+    case PHEM_ERR_TIMEOUT: return "watchdog timeout";
+    case PHEM_ERR_UNSUPPORTED: return "unsupported";
+    case PHEM_ERR_NO_DEVICE: return "no sm_100 device";
+    }
+    return "unknown status";
+}
+
+phem_status phem_context_create(int device, phem_context **out)
+{
+    if (!out) {
+        set_error("null output pointer");
+        return PHEM_ERR_INVALID;
+    }
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        set_error("device %d not available (%d CUDA devices)", device, count);
+        return PHEM_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    PHEM_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        set_error("device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+        return PHEM_ERR_NO_DEVICE;
+    }
+    DeviceGuard g(device);
+    phem_context *c = new phem_context();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    auto fail = [&](const char *what) {
+        set_error("context: %s failed: %s", what, cudaGetErrorString(cudaGetLastError()));
+        phem_context_destroy(c);
+        return PHEM_ERR_CUDA;
+    };
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail("stream");
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail("copy stream");
+    c->stream = c->own_stream;
+    if (cudaMalloc(&c->ctl, sizeof(Ctl)) != cudaSuccess)
+        return fail("control block");
+    if (cudaMallocHost(&c->h_ctl, sizeof(Ctl)) != cudaSuccess)
+        return fail("pinned control block");
+    if (cudaEventCreate(&c->ev_start) != cudaSuccess || cudaEventCreate(&c->ev_stop) != cudaSuccess)
+        return fail("events");
+    if (cudaMemset(c->ctl, 0, sizeof(Ctl)) != cudaSuccess)
+        return fail("control block init");
+    *out = c;
+    return PHEM_OK;
+}
+
+void phem_context_destroy(phem_context *ctx)
+{
+    if (!ctx)
+        return;
+    DeviceGuard g(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    if (ctx->ws)
+        cudaFree(ctx->ws);
+    if (ctx->status)
+        cudaFree(ctx->status);
+    if (ctx->ctl)
+        cudaFree(ctx->ctl);
+    if (ctx->h_ctl)
+        cudaFreeHost(ctx->h_ctl);
+    if (ctx->ev_start)
+        cudaEventDestroy(ctx->ev_start);
+    if (ctx->ev_stop)
+        cudaEventDestroy(ctx->ev_stop);
+    for (auto &p : ctx->pending) {
+        cudaEventDestroy(p.start);
+        cudaEventDestroy(p.stop);
+    }
+    for (auto e : ctx->event_pool)
+        cudaEventDestroy(e);
+    if (ctx->copy_stream)
+        cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->own_stream)
+        cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+phem_status phem_context_set_stream(phem_context *ctx, void *stream)
+{
+    PHEM_TRY(check_ctx(ctx));
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return PHEM_OK;
+}
+
+void *phem_context_stream(phem_context *ctx) { return ctx ? ctx->stream : nullptr; }
+
+phem_status phem_context_set_timeout_ms(phem_context *ctx, uint32_t ms)
+{
+    PHEM_TRY(check_ctx(ctx));
+    ctx->timeout_ms = ms;
+    return PHEM_OK;
+}
+
+phem_status phem_context_set_profiling(phem_context *ctx, int on)
+{
+    PHEM_TRY(check_ctx(ctx));
+    ctx->profiling = on != 0;
+    return PHEM_OK;
+}
+
+phem_status phem_context_profile(phem_context *ctx, phem_kernel_profile *out, uint32_t max, uint32_t *count)
+{
+    PHEM_TRY(check_ctx(ctx));
+    DeviceGuard g(ctx->device);
+    PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    resolve_timings(ctx);
+    uint32_t k = 0;
+    for (int i = 0; i < kKernelCount; i++) {
+        if (!ctx->launches[i])
+            continue;
+        if (out && k < max) {
+            std::memset(&out[k], 0, sizeof(out[k]));
+            std::snprintf(out[k].name, sizeof(out[k].name), "%s", kKernelNames[i]);
+            out[k].launches = ctx->launches[i];
+            out[k].timed_launches = ctx->timed_launches[i];
+            out[k].total_ms = ctx->kernel_ms[i];
+        }
+        k++;
+    }
+    if (count)
+        *count = k;
+    return PHEM_OK;
+}
+
+phem_status phem_context_profile_reset(phem_context *ctx)
+{
+    PHEM_TRY(check_ctx(ctx));
+    DeviceGuard g(ctx->device);
+    PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    resolve_timings(ctx);
+    for (int i = 0; i < kKernelCount; i++) {
+        ctx->launches[i] = 0;
+        ctx->timed_launches[i] = 0;
+        ctx->kernel_ms[i] = 0;
+    }
+    return PHEM_OK;
+}
+
+phem_status phem_context_trim(phem_context *ctx)
+{
+    PHEM_TRY(check_ctx(ctx));
+    DeviceGuard g(ctx->device);
+    PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->ws)
+        cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+    return PHEM_OK;
+}
+
+// ------------------------------------------------------------------ CC
+
+phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, int32_t n, int32_t *labels,
+                          uint64_t *forest, uint32_t flags, phem_cc_stats *stats)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n <= 0 || m < 0 || (m > 0 && !edges) || !labels) {
+        set_error("cc_solve: need n > 0, m >= 0, edges and labels");
+        return PHEM_ERR_INVALID;
+    }
+    const bool canonical = flags & PHEM_CC_CANONICAL;
+    if (canonical && (uint64_t)m >= (1ull << 32)) {
+        set_error("cc_solve: canonical forest needs m < 2^32");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    const size_t eb = (size_t)m * sizeof(uint64_t), lb = (size_t)n * sizeof(int32_t),
+                 fb = (size_t)n * sizeof(uint64_t);
+    // extra area: staged edges | labels | forest | parent (default path)
+    const size_t o_edges = 0, o_lab = align256(eb), o_for = o_lab + align256(lb), o_par = o_for + align256(fb);
+    const size_t extra = o_par + align256(lb);
+    size_t base = 0;
+    MsfPlan plan;
+    if (canonical) {
+        PHEM_TRY(msf_plan(ctx, kKindPacked, nullptr, (uint64_t)m, (uint32_t)n, extra, &plan, &base));
+    } else {
+        PHEM_TRY(ws_reserve(ctx, extra));
+    }
+    Staged se, sl, sf;
+    const bool aligned_dev = is_device_ptr(edges) && (((uintptr_t)edges & 15) == 0);
+    if (aligned_dev) {
+        se.dev = const_cast<uint64_t *>(edges);
+    } else {
+        se.dev = static_cast<char *>(ctx->ws) + base + o_edges;
+        if (m)
+            PHEM_CUDA_TRY(cudaMemcpyAsync(se.dev, edges, eb, cudaMemcpyDefault, ctx->stream));
+    }
+    stage_out(ctx, labels, lb, base + o_lab, &sl);
+    stage_out(ctx, forest, fb, base + o_for, &sf);
+    const uint64_t *d_edges = static_cast<const uint64_t *>(se.dev);
+    int32_t *d_lab = static_cast<int32_t *>(sl.dev);
+    uint64_t *d_for = static_cast<uint64_t *>(sf.dev);
+
+    Timed timer(ctx);
+    uint32_t rounds = 0;
+    if (canonical) {
+        plan.e0 = d_edges;
+        plan.forest = d_for;
+        PHEM_TRY(msf_run(ctx, kKindPacked, plan, &rounds));
+        // plan.best is free after the rounds: reuse it as the per-root min-id array
+        PHEM_TRY(cc_launch_minid_labels(ctx, n, plan.parent, reinterpret_cast<uint32_t *>(plan.best), d_lab));
+    } else {
+        int32_t *d_par = reinterpret_cast<int32_t *>(static_cast<char *>(ctx->ws) + base + o_par);
+        PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), ctx->stream));
+        PHEM_TRY(cc_launch_init(ctx, n, d_par, nullptr, d_for));
+        PHEM_TRY(cc_launch_unite(ctx, d_edges, m, n, d_par, d_for));
+        PHEM_TRY(cc_launch_label(ctx, n, d_par, d_lab));
+    }
+    const float ms = timer.stop();
+    PHEM_CUDA_TRY(cudaMemsetAsync(&ctx->ctl->misc[0], 0, 2 * sizeof(unsigned long long), ctx->stream));
+    PHEM_TRY(cc_launch_count(ctx, n, d_lab, d_for));
+    PHEM_TRY(copy_back(ctx, sl, lb));
+    PHEM_TRY(copy_back(ctx, sf, fb));
+    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    PHEM_TRY(stream_wait(ctx));
+    PHEM_TRY(ctl_status(ctx->h_ctl->err, "cc_solve"));
+    if (stats) {
+        stats->components = (uint32_t)ctx->h_ctl->misc[0];
+        stats->forest_edges = d_for ? ctx->h_ctl->misc[1] : (uint64_t)n - ctx->h_ctl->misc[0];
+        stats->rounds = rounds;
+        stats->device_ms = ms;
+    }
+    return PHEM_OK;
+}
+
+phem_status phem_cc_init(phem_context *ctx, int32_t n, int32_t *d_parent, int32_t *d_label, uint64_t *d_forest)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n <= 0 || !d_parent) {
+        set_error("cc_init: need n > 0 and a parent array");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    return cc_launch_init(ctx, n, d_parent, d_label, d_forest);
+}
+
+phem_status phem_cc_unite(phem_context *ctx, const uint64_t *d_edges, int64_t m, int32_t n, int32_t *d_parent,
+                          uint64_t *d_forest)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n <= 0 || m < 0 || !d_parent || (m > 0 && !d_edges) || ((uintptr_t)d_edges & 15)) {
+        set_error("cc_unite: need n > 0, m >= 0, 16-byte aligned device edges");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    return cc_launch_unite(ctx, d_edges, m, n, d_parent, d_forest);
+}
+
+phem_status phem_cc_label(phem_context *ctx, int32_t n, int32_t *d_parent, int32_t *d_label)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n <= 0 || !d_parent || !d_label) {
+        set_error("cc_label: need n > 0, parent and label arrays");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    return cc_launch_label(ctx, n, d_parent, d_label);
+}
+
+phem_status phem_cc_stream(phem_context *ctx, const uint64_t *h_edges, int64_t m, int32_t n, int64_t batch,
+                           int32_t *d_parent, int32_t *d_label, uint64_t *d_forest, float *ms)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n <= 0 || m < 0 || batch <= 0 || !d_parent || (m > 0 && !h_edges)) {
+        set_error("cc_stream: need n > 0, m >= 0, batch > 0, parent array");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    constexpr int kBuffers = 3;
+    const size_t bb = align256((size_t)batch * sizeof(uint64_t));
+    PHEM_TRY(ws_reserve(ctx, bb * kBuffers));
+    cudaEvent_t copied[kBuffers], freed[kBuffers];
+    for (int b = 0; b < kBuffers; b++) {
+        PHEM_CUDA_TRY(cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming));
+        PHEM_CUDA_TRY(cudaEventCreateWithFlags(&freed[b], cudaEventDisableTiming));
+    }
+    PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), ctx->stream));
+    PHEM_TRY(cc_launch_init(ctx, n, d_parent, d_label, d_forest));
+    Timed timer(ctx);
+    // Copies run on the copy stream, unions on the context stream.  Buffer b is
+    // refilled only after the union that read it has finished (freed[b]; an
+    // event that was never recorded does not block), and a union starts only
+    // after its copy (copied[b]).  The first copy waits for the timer start.
+    PHEM_CUDA_TRY(cudaEventRecord(copied[0], ctx->stream));
+    PHEM_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, copied[0], 0));
+    int64_t k = 0;
+    for (int64_t off = 0; off < m; off += batch, k++) {
+        const int b = (int)(k % kBuffers);
+        const int64_t cnt = std::min<int64_t>(batch, m - off);
+        uint64_t *buf = reinterpret_cast<uint64_t *>(static_cast<char *>(ctx->ws) + bb * b);
+        PHEM_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, freed[b], 0));
+        PHEM_CUDA_TRY(cudaMemcpyAsync(buf, h_edges + off, (size_t)cnt * sizeof(uint64_t), cudaMemcpyDefault,
+                                      ctx->copy_stream));
+        PHEM_CUDA_TRY(cudaEventRecord(copied[b], ctx->copy_stream));
+        PHEM_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, copied[b], 0));
+        PHEM_TRY(cc_launch_unite(ctx, buf, cnt, n, d_parent, d_forest));
+        PHEM_CUDA_TRY(cudaEventRecord(freed[b], ctx->stream));
+    }
+    const float t = timer.stop();
+    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    phem_status st = stream_wait(ctx);
+    for (int b = 0; b < kBuffers; b++) {
+        cudaEventDestroy(copied[b]);
+        cudaEventDestroy(freed[b]);
+    }
+    PHEM_TRY(st);
+    PHEM_TRY(ctl_status(ctx->h_ctl->err, "cc_stream"));
+    if (ms)
+        *ms = t;
+    return PHEM_OK;
+}
+
+phem_status phem_cc_merge(phem_context *ctx, const uint64_t *d_forest_a, const uint64_t *d_forest_b, int32_t n,
+                          int32_t *d_parent, int32_t *d_label, uint64_t *d_forest_out, float *ms)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n <= 0 || !d_forest_a || !d_parent || !d_label) {
+        set_error("cc_merge: need n > 0, forest_a, parent and label arrays");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), ctx->stream));
+    PHEM_TRY(cc_launch_init(ctx, n, d_parent, d_label, d_forest_out));
+    Timed timer(ctx);
+    PHEM_TRY(cc_launch_merge(ctx, d_forest_a, d_forest_b, n, d_parent, d_forest_out));
+    PHEM_TRY(cc_launch_label(ctx, n, d_parent, d_label));
+    const float t = timer.stop();
+    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    PHEM_TRY(stream_wait(ctx));
+    PHEM_TRY(ctl_status(ctx->h_ctl->err, "cc_merge"));
+    if (ms)
+        *ms = t;
+    return PHEM_OK;
+}
+
+// ------------------------------------------------------------------ MSF
+
+static phem_status msf_common(phem_context *ctx, const phem_edge *edges, uint64_t m, uint32_t n, phem_edge *msf,
+                              uint64_t *count, uint64_t *total, phem_msf_stats *stats, uint64_t *d_count_total)
+{
+    if (n == 0 || n == UINT32_MAX || m >= (1ull << 32) || (m > 0 && !edges)) {
+        set_error("msf: need 0 < n < 2^32 - 1, m < 2^32 and an edge array");
+        return PHEM_ERR_INVALID;
+    }
+    const size_t eb = (size_t)m * sizeof(phem_edge), ob = (size_t)n * sizeof(phem_edge);
+    const size_t o_edges = 0, o_out = align256(eb);
+    size_t base = 0;
+    MsfPlan plan;
+    PHEM_TRY(msf_plan(ctx, kKindMsf, nullptr, m, n, o_out + align256(ob), &plan, &base));
+    Staged se, so;
+    const bool aligned_dev = is_device_ptr(edges) && (((uintptr_t)edges & 15) == 0);
+    if (aligned_dev) {
+        se.dev = const_cast<phem_edge *>(edges);
+    } else {
+        se.dev = static_cast<char *>(ctx->ws) + base + o_edges;
+        if (m)
+            PHEM_CUDA_TRY(cudaMemcpyAsync(se.dev, edges, eb, cudaMemcpyDefault, ctx->stream));
+    }
+    stage_out(ctx, msf, ob, base + o_out, &so);
+    plan.e0 = se.dev;
+    Timed timer(ctx);
+    uint32_t rounds = 0;
+    PHEM_TRY(msf_run(ctx, kKindMsf, plan, &rounds));
+    PHEM_TRY(msf_gather(ctx, plan, static_cast<phem_edge *>(so.dev)));
+    const float ms = timer.stop();
+    if (d_count_total)
+        PHEM_CUDA_TRY(cudaMemcpyAsync(d_count_total, &ctx->ctl->msf_count, 2 * sizeof(uint64_t),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    PHEM_TRY(stream_wait(ctx));
+    const Ctl &h = *ctx->h_ctl;
+    PHEM_TRY(ctl_status(h.err, "msf"));
+    if (h.msf_count > (uint64_t)n - 1 + (n == 0)) {
+        set_error("msf: %llu forest edges for %u vertices", (unsigned long long)h.msf_count, n);
+        return PHEM_ERR_NONCONVERGED;
+    }
+    if (so.host && h.msf_count)
+        PHEM_CUDA_TRY(cudaMemcpy(so.host, so.dev, h.msf_count * sizeof(phem_edge), cudaMemcpyDeviceToHost));
+    if (count)
+        *count = h.msf_count;
+    if (total)
+        *total = h.msf_total;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->rounds = rounds;
+        for (uint32_t r = 0; r < rounds && r < PHEM_MAX_ROUNDS; r++) {
+            stats->m_r[r] = h.m_r[r];
+            stats->n_r[r] = h.n_r[r];
+        }
+        stats->msf_edges = h.msf_count;
+        stats->total_weight = h.msf_total;
+        stats->device_ms = ms;
+    }
+    return PHEM_OK;
+}
+
+phem_status phem_msf_solve(phem_context *ctx, const phem_edge *edges, uint64_t m, uint32_t n, phem_edge *msf,
+                           uint64_t *count, uint64_t *total, phem_msf_stats *stats)
+{
+    PHEM_TRY(check_ctx(ctx));
+    DeviceGuard g(ctx->device);
+    return msf_common(ctx, edges, m, n, msf, count, total, stats, nullptr);
+}
+
+phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, uint64_t m, uint32_t n,
+                                  phem_edge *d_msf, uint64_t *d_count_total, phem_msf_stats *stats)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (!is_device_ptr(d_edges) || (d_msf && !is_device_ptr(d_msf)) ||
+        (d_count_total && !is_device_ptr(d_count_total))) {
+        set_error("msf_solve_device: arrays must be device memory");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    return msf_common(ctx, d_edges, m, n, d_msf, nullptr, nullptr, stats, d_count_total);
+}
+
+phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, uint32_t n,
+                               const uint32_t *weights, uint64_t m_upper, phem_edge *msf, uint64_t *count,
+                               uint64_t *total, phem_msf_stats *stats)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n == 0 || n >= (1u << 31) || !offsets || m_upper >= (1ull << 32) || (m_upper > 0 && (!cols || !weights))) {
+        set_error("msf_solve_csr: need 0 < n < 2^31, offsets, cols, weights, m_upper < 2^32");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    int64_t nnz = 0;
+    PHEM_CUDA_TRY(cudaMemcpyAsync(&nnz, offsets + n, sizeof(int64_t), cudaMemcpyDefault, ctx->stream));
+    PHEM_TRY(stream_wait(ctx));
+    if (nnz < 0 || (uint64_t)nnz >= (1ull << 32)) {
+        set_error("msf_solve_csr: offsets[n] = %lld out of range", (long long)nnz);
+        return PHEM_ERR_INVALID;
+    }
+    // The converted edge list lives in a device buffer of its own so the MSF
+    // solve can size the workspace freely.
+    const size_t ob = (size_t)(n + 1) * sizeof(int64_t), cb = (size_t)nnz * sizeof(uint32_t),
+                 pb = (size_t)nnz * sizeof(uint64_t), wb = (size_t)m_upper * sizeof(uint32_t),
+                 rb = (size_t)m_upper * sizeof(phem_edge);
+    const size_t o_off = 0, o_col = align256(ob), o_w = o_col + align256(cb), o_pk = o_w + align256(wb),
+                 o_rec = o_pk + align256(pb);
+    void *buf = nullptr;
+    if (cudaMalloc(&buf, o_rec + align256(rb) + 256) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("msf_solve_csr: cannot allocate the edge list");
+        return PHEM_ERR_NOMEM;
+    }
+    char *b = static_cast<char *>(buf);
+    auto put = [&](const void *src, size_t bytes, size_t off) -> const void * {
+        if (is_device_ptr(src))
+            return src;
+        if (bytes)
+            cudaMemcpyAsync(b + off, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+        return b + off;
+    };
+    const int64_t *d_off = static_cast<const int64_t *>(put(offsets, ob, o_off));
+    const uint32_t *d_col = static_cast<const uint32_t *>(put(cols, cb, o_col));
+    const uint32_t *d_w = static_cast<const uint32_t *>(put(weights, wb, o_w));
+    uint64_t *d_pk = reinterpret_cast<uint64_t *>(b + o_pk);
+    phem_edge *d_rec = reinterpret_cast<phem_edge *>(b + o_rec);
+    phem_status st = csr_launch_to_coo(ctx, d_off, d_col, (int32_t)n, nnz, d_pk);
+    if (st == PHEM_OK && cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost,
+                                         ctx->stream) != cudaSuccess)
+        st = PHEM_ERR_CUDA;
+    if (st == PHEM_OK)
+        st = stream_wait(ctx);
+    if (st == PHEM_OK)
+        st = ctl_status(ctx->h_ctl->err, "msf_solve_csr");
+    if (st == PHEM_OK && ctx->h_ctl->misc[2] != m_upper) {
+        set_error("msf_solve_csr: CSR has %llu entries with row < col, m_upper = %llu",
+                  (unsigned long long)ctx->h_ctl->misc[2], (unsigned long long)m_upper);
+        st = PHEM_ERR_INVALID;
+    }
+    if (st == PHEM_OK)
+        st = csr_launch_pack_records(ctx, d_pk, d_w, m_upper, d_rec);
+    if (st == PHEM_OK)
+        st = msf_common(ctx, d_rec, m_upper, n, msf, count, total, stats, nullptr);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(buf);
+    return st;
+}
+
+phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, int32_t n,
+                            uint64_t *out, int64_t *out_m)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (n <= 0 || !offsets || !out_m) {
+        set_error("csr_to_coo: need n > 0, offsets and out_m");
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    int64_t nnz = 0;
+    PHEM_CUDA_TRY(cudaMemcpyAsync(&nnz, offsets + n, sizeof(int64_t), cudaMemcpyDefault, ctx->stream));
+    PHEM_TRY(stream_wait(ctx));
+    if (nnz < 0 || (nnz > 0 && !cols)) {
+        set_error("csr_to_coo: bad offsets[n] = %lld", (long long)nnz);
+        return PHEM_ERR_INVALID;
+    }
+    const size_t ob = (size_t)(n + 1) * sizeof(int64_t), cb = (size_t)nnz * sizeof(uint32_t),
+                 xb = (size_t)nnz * sizeof(uint64_t);
+    const size_t o_off = 0, o_col = align256(ob), o_out = o_col + align256(cb);
+    PHEM_TRY(ws_reserve(ctx, o_out + align256(xb / 2 + 16)));
+    Staged so, sc, sx;
+    PHEM_TRY(stage_in(ctx, offsets, ob, o_off, &so));
+    PHEM_TRY(stage_in(ctx, cols, cb, o_col, &sc));
+    stage_out(ctx, out, 0, o_out, &sx);
+    // host output: stage only as much as can be kept (at most nnz / 2 entries have row < col
+    // in a symmetric CSR; a non-symmetric one may keep more, so count first in that case)
+    if (sx.host) {
+        PHEM_TRY(csr_launch_to_coo(ctx, static_cast<const int64_t *>(so.dev), static_cast<const uint32_t *>(sc.dev),
+                                   n, nnz, nullptr));
+        PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+        PHEM_TRY(stream_wait(ctx));
+        const uint64_t kept = ctx->h_ctl->misc[2];
+        if (kept > xb / 2 / sizeof(uint64_t) + 2) {
+            // grow: the workspace is reallocated, so stage the inputs again
+            PHEM_TRY(ws_reserve(ctx, o_out + align256(kept * sizeof(uint64_t))));
+            PHEM_TRY(stage_in(ctx, offsets, ob, o_off, &so));
+            PHEM_TRY(stage_in(ctx, cols, cb, o_col, &sc));
+            stage_out(ctx, out, 0, o_out, &sx);
+        }
+    }
+    PHEM_TRY(csr_launch_to_coo(ctx, static_cast<const int64_t *>(so.dev), static_cast<const uint32_t *>(sc.dev), n,
+                               nnz, static_cast<uint64_t *>(sx.dev)));
+    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    PHEM_TRY(stream_wait(ctx));
+    PHEM_TRY(ctl_status(ctx->h_ctl->err, "csr_to_coo"));
+    const uint64_t kept = ctx->h_ctl->misc[2];
+    if (sx.host && kept)
+        PHEM_CUDA_TRY(cudaMemcpy(sx.host, sx.dev, kept * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    *out_m = (int64_t)kept;
+    return PHEM_OK;
+}
+
+}  // extern "C"

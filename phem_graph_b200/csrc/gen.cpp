@@ -1,0 +1,274 @@
+// gen.cpp -- seeded synthetic graph generators (host side).
+//
+// The reference benchmarks on files that are not shipped with it; these
+// generators stand in for them with seeded inputs of the same shapes.  Every
+// random value is a pure function of (seed, stream tag, counter): SplitMix64
+// (Steele, Lea, Flood, "Fast splittable pseudorandom number generators",
+// OOPSLA 2014) evaluated at counter i, reduced to a range with Lemire's
+// multiply-shift.  Output is therefore identical for any thread count, and the
+// CPU oracle and the GPU tests see the same graphs.
+//
+// Edge formats produced:
+//   - packed CC edges: uint64 (u << 32 | v) with u < v, the format
+//     CC/graph.cu:76,176 builds;
+//   - MSF edges: {u, v, w} uint32 records (MST/src/constants.h:15-19);
+//   - symmetrised CSR: int64 offsets[n + 1], uint32 cols[2m], rows sorted by
+//     column (the ECL .egr layout read by CC/graph.cu:90-121).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../../include/phem.h"
+
+namespace {
+
+constexpr uint64_t kGamma = 0x9E3779B97F4A7C15ull;
+
+inline uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Base of the stream `tag` under `seed`; value i of the stream is
+// mix64(base + (i + 1) * gamma), i.e. the i-th output of a SplitMix64
+// generator whose state starts at base.
+inline uint64_t stream_base(uint64_t seed, uint64_t tag) { return mix64(seed * kGamma + tag); }
+inline uint64_t stream_at(uint64_t base, uint64_t i) { return mix64(base + (i + 1) * kGamma); }
+inline uint32_t lemire(uint32_t x, uint32_t range) { return (uint32_t)(((uint64_t)x * range) >> 32); }
+
+constexpr uint64_t kTagER = 0x45522D45444745ull;    // "ER-EDGE"
+constexpr uint64_t kTagRMAT = 0x524D41542D4544ull;  // "RMAT-ED"
+constexpr uint64_t kTagW = 0x5745494748542Dull;     // "WEIGHT-"
+
+int num_threads()
+{
+    unsigned t = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(t, 64u));
+}
+
+template <class F>
+void parallel_ranges(uint64_t count, F &&f)
+{
+    int T = num_threads();
+    if (count < (1u << 16))
+        T = 1;
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; t++) {
+        uint64_t lo = count * t / T, hi = count * (t + 1) / T;
+        pool.emplace_back([&, t, lo, hi] { f(t, lo, hi); });
+    }
+    for (auto &th : pool)
+        th.join();
+}
+
+// Generic two-pass "emit if" over draws [0, draws): produce(i, &value) returns
+// whether draw i yields a value.  Output keeps draw order.
+template <class P>
+uint64_t emit_in_draw_order(uint64_t draws, uint64_t *out, P &&produce)
+{
+    int T = (draws < (1u << 16)) ? 1 : num_threads();
+    std::vector<uint64_t> counts(T + 1, 0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; t++)
+        pool.emplace_back([&, t] {
+            uint64_t lo = draws * t / T, hi = draws * (t + 1) / T, c = 0, v;
+            for (uint64_t i = lo; i < hi; i++)
+                c += produce(i, &v) ? 1 : 0;
+            counts[t + 1] = c;
+        });
+    for (auto &th : pool)
+        th.join();
+    pool.clear();
+    for (int t = 0; t < T; t++)
+        counts[t + 1] += counts[t];
+    if (out)
+        for (int t = 0; t < T; t++)
+            pool.emplace_back([&, t] {
+                uint64_t lo = draws * t / T, hi = draws * (t + 1) / T, k = counts[t], v;
+                for (uint64_t i = lo; i < hi; i++)
+                    if (produce(i, &v))
+                        out[k++] = v;
+            });
+    for (auto &th : pool)
+        th.join();
+    return counts[T];
+}
+
+// Parallel LSD radix sort of keys that fit in `bits` bits, 11-bit digits.
+void radix_sort(uint64_t *keys, uint64_t count, int bits)
+{
+    if (count < 2)
+        return;
+    constexpr int D = 11, B = 1 << D;
+    std::vector<uint64_t> tmp(count);
+    uint64_t *src = keys, *dst = tmp.data();
+    int T = (count < (1u << 18)) ? 1 : num_threads();
+    std::vector<uint64_t> hist((size_t)T * B);
+    for (int shift = 0; shift < bits; shift += D) {
+        std::fill(hist.begin(), hist.end(), 0);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; t++)
+            pool.emplace_back([&, t] {
+                uint64_t lo = count * t / T, hi = count * (t + 1) / T;
+                uint64_t *h = &hist[(size_t)t * B];
+                for (uint64_t i = lo; i < hi; i++)
+                    h[(src[i] >> shift) & (B - 1)]++;
+            });
+        for (auto &th : pool)
+            th.join();
+        pool.clear();
+        uint64_t sum = 0;
+        for (int d = 0; d < B; d++)
+            for (int t = 0; t < T; t++) {
+                uint64_t c = hist[(size_t)t * B + d];
+                hist[(size_t)t * B + d] = sum;
+                sum += c;
+            }
+        for (int t = 0; t < T; t++)
+            pool.emplace_back([&, t] {
+                uint64_t lo = count * t / T, hi = count * (t + 1) / T;
+                uint64_t *h = &hist[(size_t)t * B];
+                for (uint64_t i = lo; i < hi; i++)
+                    dst[h[(src[i] >> shift) & (B - 1)]++] = src[i];
+            });
+        for (auto &th : pool)
+            th.join();
+        std::swap(src, dst);
+    }
+    if (src != keys)
+        std::memcpy(keys, src, count * sizeof(uint64_t));
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t phem_gen_mix64(uint64_t seed, uint64_t tag, uint64_t i)
+{
+    return stream_at(stream_base(seed, tag), i);
+}
+
+phem_status phem_gen_er(uint32_t n, uint64_t draws, uint64_t seed, uint64_t *out, uint64_t *out_m)
+{
+    if (n < 2 || !out_m)
+        return PHEM_ERR_INVALID;
+    const uint64_t base = stream_base(seed, kTagER);
+    *out_m = emit_in_draw_order(draws, out, [&](uint64_t i, uint64_t *val) {
+        uint64_t r = stream_at(base, i);
+        uint32_t a = lemire((uint32_t)(r >> 32), n), b = lemire((uint32_t)r, n);
+        if (a == b)
+            return false;  // self-loops are dropped, duplicates kept
+        uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+        *val = ((uint64_t)lo << 32) | hi;
+        return true;
+    });
+    return PHEM_OK;
+}
+
+phem_status phem_gen_rmat(uint32_t scale, uint64_t draws, double a, double b, double c, uint64_t seed,
+                          uint64_t *out, uint64_t *out_m)
+{
+    if (scale < 1 || scale > 31 || !out_m || a < 0 || b < 0 || c < 0 || a + b + c > 1.0)
+        return PHEM_ERR_INVALID;
+    const uint64_t base = stream_base(seed, kTagRMAT);
+    const uint32_t words = (scale + 1) / 2;
+    const double two32 = 4294967296.0;
+    const uint64_t tA = (uint64_t)std::floor(a * two32);
+    const uint64_t tAB = (uint64_t)std::floor((a + b) * two32);
+    const uint64_t tABC = (uint64_t)std::floor((a + b + c) * two32);
+    // Pairs are emitted compactly as (lo << scale | hi) so the sort runs on 2*scale bits.
+    uint64_t m = emit_in_draw_order(draws, out, [&](uint64_t i, uint64_t *val) {
+        uint32_t u = 0, v = 0;
+        for (uint32_t l = 0; l < scale; l++) {
+            uint64_t word = stream_at(base, i * words + l / 2);
+            uint64_t r = (l & 1) ? (word >> 32) : (word & 0xffffffffu);
+            uint32_t ubit = r >= tAB;                       // quadrants c, d
+            uint32_t vbit = (r >= tA && r < tAB) || r >= tABC;  // quadrants b, d
+            u = (u << 1) | ubit;
+            v = (v << 1) | vbit;
+        }
+        if (u == v)
+            return false;
+        uint64_t lo = u < v ? u : v, hi = u < v ? v : u;
+        *val = (lo << scale) | hi;
+        return true;
+    });
+    if (out) {
+        radix_sort(out, m, 2 * (int)scale);
+        const uint64_t mask = (1ull << scale) - 1;
+        parallel_ranges(m, [&](int, uint64_t lo, uint64_t hi) {
+            for (uint64_t i = lo; i < hi; i++)
+                out[i] = ((out[i] >> scale) << 32) | (out[i] & mask);
+        });
+    }
+    *out_m = m;
+    return PHEM_OK;
+}
+
+phem_status phem_gen_weights(uint64_t m, uint64_t seed, uint32_t bits, uint32_t *w)
+{
+    if (!w || bits < 1 || bits > 31)
+        return PHEM_ERR_INVALID;
+    const uint64_t base = stream_base(seed, kTagW);
+    const uint64_t mask = (1ull << bits) - 1;
+    parallel_ranges(m, [&](int, uint64_t lo, uint64_t hi) {
+        for (uint64_t i = lo; i < hi; i++)
+            w[i] = (uint32_t)(1 + (stream_at(base, i) & mask));
+    });
+    return PHEM_OK;
+}
+
+phem_status phem_pack_msf_edges(const uint64_t *pairs, const uint32_t *w, uint64_t m, phem_edge *out)
+{
+    if (!pairs || !out)
+        return PHEM_ERR_INVALID;
+    parallel_ranges(m, [&](int, uint64_t lo, uint64_t hi) {
+        for (uint64_t i = lo; i < hi; i++) {
+            out[i].u = (uint32_t)(pairs[i] >> 32);
+            out[i].v = (uint32_t)pairs[i];
+            out[i].w = w ? w[i] : 0;
+        }
+    });
+    return PHEM_OK;
+}
+
+// Symmetrised CSR from pairs sorted by (u, v) with u < v: row x holds every
+// partner of x, ascending (partners below x come from pairs (y, x), those above
+// from pairs (x, y)), duplicates kept.  offsets has n + 1 entries, cols 2m.
+phem_status phem_csr_from_sorted_pairs(const uint64_t *pairs, uint64_t m, uint32_t n, int64_t *offsets,
+                                       uint32_t *cols)
+{
+    if (!pairs || !offsets || !cols)
+        return PHEM_ERR_INVALID;
+    std::vector<uint64_t> low(n + 1, 0), high(n + 1, 0);  // partners below / above each row
+    for (uint64_t i = 0; i < m; i++) {
+        uint32_t u = (uint32_t)(pairs[i] >> 32), v = (uint32_t)pairs[i];
+        if (u >= v || v >= n)
+            return PHEM_ERR_INVALID;
+        high[u]++;
+        low[v]++;
+    }
+    offsets[0] = 0;
+    for (uint32_t x = 0; x < n; x++)
+        offsets[x + 1] = offsets[x] + (int64_t)(low[x] + high[x]);
+    // fill cursors: partners below x land first, in increasing y because pairs are sorted by u
+    std::vector<int64_t> lowpos(n), highpos(n);
+    for (uint32_t x = 0; x < n; x++) {
+        lowpos[x] = offsets[x];
+        highpos[x] = offsets[x] + (int64_t)low[x];
+    }
+    for (uint64_t i = 0; i < m; i++) {
+        uint32_t u = (uint32_t)(pairs[i] >> 32), v = (uint32_t)pairs[i];
+        cols[lowpos[v]++] = u;
+        cols[highpos[u]++] = v;
+    }
+    return PHEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+// internal.h -- host-side internals shared by the library's translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/phem.h"
+#include "common.cuh"
+
+namespace phem {
+// Kernels the library launches; the profile reports them by these names.
+enum KernelId : int {
+    kKInit = 0, kKRound0, kKEdgePass, kKHook, kKCompress, kKAdvance, kKGather,
+    kKCcInit, kKCcUnite, kKCcMerge, kKCcLabel, kKMinid, kKCcCount, kKCsrCoo, kKPack,
+    kKernelCount
+};
+extern const char *const kKernelNames[kKernelCount];
+
+struct PendingTiming {
+    int kernel;
+    cudaEvent_t start, stop;
+};
+}  // namespace phem
+
+struct phem_context {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;     // stream the work is ordered on
+    cudaStream_t own_stream = nullptr; // stream created with the context
+    cudaStream_t copy_stream = nullptr;// second stream for overlapped host copies
+    void *ws = nullptr;                // grow-only device workspace
+    size_t ws_bytes = 0;
+    uint64_t *status = nullptr;        // look-back status words, only ever written by look-back
+    size_t status_words = 0;           // (zeroed when grown; epochs keep old words from matching)
+    phem::Ctl *ctl = nullptr;          // device control block
+    phem::Ctl *h_ctl = nullptr;        // pinned host mirror of the control block
+    uint64_t epoch = 1;                // look-back epoch counter
+    uint32_t timeout_ms = 0;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    int edge_pass_blocks = 0;          // persistent grid sizes, from the occupancy API
+    int round0_blocks = 0;
+    int gather_blocks = 0;
+    // launch accounting and optional per-kernel CUDA-event timing
+    uint64_t launches[phem::kKernelCount] = {};
+    double kernel_ms[phem::kKernelCount] = {};
+    uint64_t timed_launches[phem::kKernelCount] = {};
+    bool profiling = false;
+    std::vector<phem::PendingTiming> pending;
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace phem {
+
+// Thread-local last-error text.
+void set_error(const char *fmt, ...);
+
+// CUDA call check: records the failure and returns PHEM_ERR_CUDA.
+#define PHEM_CUDA_TRY(call)                                                                 \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            ::phem::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return PHEM_ERR_CUDA;                                                           \
+        }                                                                                   \
+    } while (0)
+
+#define PHEM_TRY(expr)                       \
+    do {                                     \
+        phem_status s_ = (expr);             \
+        if (s_ != PHEM_OK)                   \
+            return s_;                       \
+    } while (0)
+
+// Carves 256-byte aligned sub-buffers out of the context workspace.
+struct Carve {
+    size_t off = 0;
+    template <class T>
+    size_t take(size_t count)
+    {
+        size_t at = (off + 255) & ~size_t(255);
+        off = at + count * sizeof(T);
+        return at;
+    }
+};
+
+// Ensures ws_bytes >= bytes (contents are not preserved when it grows).
+phem_status ws_reserve(phem_context *ctx, size_t bytes);
+// Ensures the look-back status array holds >= words entries.
+phem_status status_reserve(phem_context *ctx, size_t words);
+
+// Waits for the stream, honouring the context watchdog.
+phem_status stream_wait(phem_context *ctx);
+
+// Maps the control block's error bits to a status (and the last-error text).
+phem_status ctl_status(uint32_t err, const char *what);
+
+// True when p is device (or managed) memory of the current device.
+bool is_device_ptr(const void *p);
+
+uint64_t next_epochs(phem_context *ctx, uint32_t count);
+
+// Brackets one kernel launch: counts it and, when profiling is on, records a
+// pair of events on the context stream around it.
+struct KernelScope {
+    phem_context *ctx;
+    int kernel;
+    cudaEvent_t start = nullptr;
+    KernelScope(phem_context *c, int k);
+    ~KernelScope();
+};
+// Folds finished event pairs into the per-kernel totals (call after a sync).
+void resolve_timings(phem_context *ctx);
+
+// ---- MSF engine (msf.cu) ----
+enum EdgeKind : int { kKindMsf = 0, kKindPacked = 1 };
+
+struct MsfPlan {
+    // device buffers (all inside the context workspace)
+    const void *e0;          // input records: phem_edge (kKindMsf) or packed uint64 (kKindPacked)
+    uint64_t m;
+    uint32_t n;
+    uint32_t *parent;        // n
+    unsigned long long *best;// n
+    uint32_t *cand[2];       // n each
+    uint32_t *bitmap;        // ceil(m / 32)
+    uint4 *wl[2];            // m each
+    uint64_t *status;        // look-back status (context-owned), >= tiles
+    uint64_t epoch_base;
+    uint64_t *forest;        // kKindPacked only: forest slot per hooked root (may be null)
+};
+
+size_t msf_workspace_bytes(uint64_t m, uint32_t n);
+phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, uint32_t n, size_t extra_bytes,
+                     MsfPlan *plan, size_t *extra_off);
+// Queues the whole Boruvka solve; returns after the rounds are done (host
+// checks the round flag between rounds).  On return the bitmap marks the MSF.
+phem_status msf_run(phem_context *ctx, int kind, MsfPlan &plan, uint32_t *rounds_out);
+// Queues the ordered gather of MSF edges (kKindMsf): out[0..count) + count/total into ctl.
+phem_status msf_gather(phem_context *ctx, MsfPlan &plan, phem_edge *d_out);
+
+// ---- CC engine (cc.cu) ----
+phem_status cc_launch_init(phem_context *ctx, int32_t n, int32_t *parent, int32_t *label, uint64_t *forest);
+phem_status cc_launch_unite(phem_context *ctx, const uint64_t *edges, int64_t m, int32_t n, int32_t *parent,
+                            uint64_t *forest);
+phem_status cc_launch_label(phem_context *ctx, int32_t n, int32_t *parent, int32_t *label);
+phem_status cc_launch_merge(phem_context *ctx, const uint64_t *fa, const uint64_t *fb, int32_t n, int32_t *parent,
+                            uint64_t *forest_out);
+// min-id labels from an arbitrary-root parent array (canonical forest path)
+phem_status cc_launch_minid_labels(phem_context *ctx, int32_t n, uint32_t *parent, uint32_t *minid,
+                                   int32_t *label);
+phem_status cc_launch_count(phem_context *ctx, int32_t n, const int32_t *label, const uint64_t *forest);
+
+// ---- CSR (csr.cu) ----
+// Queues the conversion of a device CSR with nnz entries; the kept count lands
+// in ctx->ctl->misc[2].
+phem_status csr_launch_to_coo(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, int32_t n,
+                              int64_t nnz, uint64_t *out);
+// {u, v, w} records from packed pairs and per-edge weights.
+phem_status csr_launch_pack_records(phem_context *ctx, const uint64_t *pairs, const uint32_t *w, uint64_t m,
+                                    phem_edge *out);
+
+}  // namespace phem

@@ -1,0 +1,133 @@
+"""GPU parity: minimum spanning forest against the reference's golden vectors
+and the oracle.  Bit-exact: the MSF edge records (ascending by edge id, as the
+PBBS result), their count and the uint64 total weight."""
+import numpy as np
+import pytest
+
+import oracle
+import phem_graph_b200 as P
+from phem_graph_b200 import _lib, gen
+from tests.golden import load, names
+
+pytestmark = pytest.mark.gpu
+MSF_CASES = names("msf_")
+
+
+def expect(E, n):
+    flags, cnt, tot = oracle.msf_kruskal(E, n)
+    return np.nonzero(flags)[0], cnt, tot
+
+
+def assert_msf(r, E, ids, cnt, tot):
+    assert r.count == cnt and r.total == tot
+    np.testing.assert_array_equal(r.edges, np.asarray(E, np.uint32).reshape(-1, 3)[ids])
+
+
+@pytest.mark.parametrize("name", MSF_CASES)
+def test_golden(ctx, name):
+    g = load(name)
+    E, n = g["edges"], int(g["n"])
+    r = ctx.msf_solve(E, n)
+    assert_msf(r, E, g["msf_ids"], int(g["count"]), int(g["total"]))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+@pytest.mark.parametrize("scale,ef,bits", [(10, 4, 20), (12, 16, 20), (14, 8, 4), (16, 16, 20), (13, 2, 1)])
+def test_rmat_random(ctx, seed, scale, ef, bits):
+    g = gen.rmat_graph(scale, ef, seed=seed, bits=bits)
+    E = g.msf_edges()
+    ids, cnt, tot = expect(E, g.n)
+    r = ctx.msf_solve(E, g.n)
+    assert_msf(r, E, ids, cnt, tot)
+    # per-round live counts equal the Boruvka restatement's
+    _, _, _, m_r, n_r = oracle.msf_boruvka(E, g.n)
+    assert r.m_r == [int(x) for x in m_r]
+    assert r.n_r == [int(x) for x in n_r]
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_er_with_ties_and_duplicates(ctx, seed):
+    p = gen.er(5000, 60000, seed)
+    p = np.concatenate([p, p[::3]])  # explicit parallel duplicates
+    E = gen.msf_edges(p, gen.weights(len(p), seed, bits=2))
+    ids, cnt, tot = expect(E, 5000)
+    assert_msf(ctx.msf_solve(E, 5000), E, ids, cnt, tot)
+
+
+@pytest.mark.slow
+def test_full_size_rmat22(ctx):
+    """The MSF workload at full size (R-MAT scale 22, edge factor 16): count,
+    total and every record against the oracle, per-round live counts against
+    the Boruvka restatement."""
+    g = gen.rmat_graph(22, 16, seed=22)
+    E = g.msf_edges()
+    flags, cnt, tot, m_r, n_r = oracle.msf_boruvka(E, g.n)
+    r = ctx.msf_solve(E, g.n)
+    assert_msf(r, E, np.nonzero(flags)[0], cnt, tot)
+    assert r.m_r == [int(x) for x in m_r] and r.n_r == [int(x) for x in n_r]
+    # idempotence: the MSF of the MSF is itself
+    r2 = ctx.msf_solve(r.edges, g.n)
+    assert (r2.count, r2.total) == (r.count, r.total)
+
+
+def test_edge_cases(ctx):
+    # no edges: empty forest
+    r = ctx.msf_solve(np.zeros((0, 3), np.uint32), 4)
+    assert (r.count, r.total) == (0, 0)
+    # only self-loops
+    r = ctx.msf_solve(np.array([[1, 1, 5], [2, 2, 1]], np.uint32), 3)
+    assert (r.count, r.total) == (0, 0)
+    # u > v and a weight of 2^31 - 1 (largest the reference's int weights hold)
+    E = np.array([[1, 0, 2**31 - 1], [2, 1, 3], [0, 2, 7]], np.uint32)
+    r = ctx.msf_solve(E, 3)
+    assert r.count == 2 and r.total == 10
+    # one vertex
+    assert ctx.msf_solve(np.zeros((0, 3), np.uint32), 1).count == 0
+    # sizes not a multiple of the 4-record vector groups
+    for m in (1, 2, 3, 5, 1023, 1025):
+        p = gen.er(64, m + 8, m)[:m]
+        E = gen.msf_edges(p, gen.weights(len(p), m, bits=3))
+        ids, cnt, tot = expect(E, 64)
+        assert_msf(ctx.msf_solve(E, 64), E, ids, cnt, tot)
+
+
+def test_out_of_range_endpoint_rejected(ctx):
+    with pytest.raises(P.PhemError) as ei:
+        ctx.msf_solve(np.array([[0, 9, 1]], np.uint32), 4)
+    assert ei.value.status == _lib.PHEM_ERR_INVALID
+    assert ctx.msf_solve(np.array([[0, 1, 1]], np.uint32), 2).count == 1
+
+
+def test_device_resident(ctx):
+    import torch
+    g = gen.rmat_graph(14, 16, seed=7)
+    E = g.msf_edges()
+    d = torch.from_numpy(E.view(np.int32)).cuda()
+    d_out = torch.empty((g.n, 3), dtype=torch.int32, device="cuda")
+    d_ct = torch.zeros(2, dtype=torch.int64, device="cuda")
+    r = ctx.msf_solve_device(d, len(E), g.n, d_out, d_ct)
+    ids, cnt, tot = expect(E, g.n)
+    ct = d_ct.cpu().numpy()
+    assert (int(ct[0]), int(ct[1])) == (cnt, tot) == (r.count, r.total)
+    np.testing.assert_array_equal(d_out[:cnt].cpu().numpy().view(np.uint32), E[ids])
+
+
+def test_csr_input(ctx):
+    """Symmetrised CSR in, edge ids numbered as csr_to_coo numbers them."""
+    g = gen.rmat_graph(13, 16, seed=3)
+    off, cols = gen.csr_from_pairs(g.pairs, g.n)
+    np.testing.assert_array_equal(ctx.csr_to_coo(off, cols, g.n), g.pairs)
+    np.testing.assert_array_equal(ctx.csr_to_coo(off, cols, g.n), oracle.csr_to_coo(off, cols, g.n))
+    E = g.msf_edges()
+    ids, cnt, tot = expect(E, g.n)
+    r = ctx.msf_solve_csr(off, cols, g.n, g.w, g.m)
+    assert_msf(r, E, ids, cnt, tot)
+
+
+def test_repeated_solves_share_context(ctx):
+    """Workspace reuse across sizes, both directions."""
+    for scale in (14, 10, 15, 9):
+        g = gen.rmat_graph(scale, 8, seed=scale)
+        E = g.msf_edges()
+        ids, cnt, tot = expect(E, g.n)
+        assert_msf(ctx.msf_solve(E, g.n), E, ids, cnt, tot)
