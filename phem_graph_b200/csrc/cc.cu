@@ -23,14 +23,14 @@
 namespace phem {
 namespace {
 
-constexpr uint32_t kFindCap = 1u << 26;
-
 // Root of x with path halving.  Writes only touch non-roots (a vertex that is
 // not a root never becomes one again), so they cannot race with the CAS that
-// hooks a root; each write points a vertex at one of its ancestors.
-__device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x, uint32_t *err)
+// hooks a root; each write points a vertex at one of its ancestors.  A path
+// has fewer than n + 1 vertices, so n + 1 steps bound the walk.
+__device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x, int32_t n, uint32_t *err)
 {
-    for (uint32_t steps = 0; steps < kFindCap; steps++) {
+    const uint32_t cap = (uint32_t)n + 1;
+    for (uint32_t steps = 0; steps < cap; steps++) {
         const int32_t p = __ldcg(parent + x);
         if (p == x)
             return x;
@@ -47,13 +47,15 @@ __device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x, uint32_t 
 // One union with the reference's hook rule (larger root under smaller root,
 // forest[hooked root] = edge).  Returns true when it hooked.
 __device__ __forceinline__ bool uf_unite(int32_t *parent, unsigned long long *forest, unsigned long long e,
-                                         int32_t u, int32_t v, uint32_t *err)
+                                         int32_t u, int32_t v, int32_t n, uint32_t *err)
 {
     for (uint32_t retry = 0; retry < kUnionRetryCap; retry++) {
-        const int32_t ru = uf_find(parent, u, err);
-        const int32_t rv = uf_find(parent, v, err);
+        const int32_t ru = uf_find(parent, u, n, err);
+        const int32_t rv = uf_find(parent, v, n, err);
         if (ru == rv)
             return false;
+        if ((retry & 63) == 63 && (*(volatile uint32_t *)err & (kErrChase | kErrRetry)))
+            return false;  // another thread already reported a broken state
         const int32_t hi = ru > rv ? ru : rv, lo = ru > rv ? rv : ru;
         if (atomicCAS(parent + hi, hi, lo) == hi) {
             if (forest)
@@ -77,7 +79,7 @@ __device__ __forceinline__ void unite_packed(int32_t *parent, unsigned long long
         set_err(err, kErrRange);
         return;
     }
-    uf_unite(parent, forest, e, u, v, err);
+    uf_unite(parent, forest, e, u, v, n, err);
 }
 
 __global__ void __launch_bounds__(kBlock) cc_init_kernel(int32_t n, int32_t *parent, int32_t *label,
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(kBlock) cc_label_kernel(int32_t n, int32_t *pa
 {
     const int32_t stride = gridDim.x * blockDim.x;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const int32_t r = uf_find(parent, i, err);
+        const int32_t r = uf_find(parent, i, n, err);
         label[i] = r;
         if (parent[i] != r)
             parent[i] = r;

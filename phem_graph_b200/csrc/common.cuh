@@ -26,8 +26,8 @@ constexpr int kBlock = 256;                    // threads per block for the stre
 constexpr int kWarps = kBlock / 32;
 constexpr int kItems = 4;                      // records per thread per tile
 constexpr int kTile = kBlock * kItems;         // records per tile
-constexpr uint32_t kUnionRetryCap = 1u << 22;  // CAS retries per union
-constexpr uint32_t kLookbackSpinCap = 1u << 24;
+constexpr uint32_t kUnionRetryCap = 1u << 16;  // CAS retries per union
+constexpr uint32_t kLookbackSpinCap = 1u << 20; // waits per look-back window (~1 s)
 
 // ---------------------------------------------------------------- device control block
 // Small per-context device structure, zeroed at the start of each solve.
@@ -185,7 +185,11 @@ __device__ __forceinline__ uint32_t lookback_exclusive(uint64_t *status, uint32_
         const unsigned need = incl_mask ? ((incl_mask & (0u - incl_mask)) << 1) - 1 : 0xffffffffu;
         const unsigned ready_mask = __ballot_sync(0xffffffffu, ready);
         if ((ready_mask & need) != need) {
-            if (++spins > kLookbackSpinCap) {
+            // give up at the cap, or at once when another block already gave up
+            bool give_up = ++spins > kLookbackSpinCap;
+            if (!give_up && (spins & 255) == 0)
+                give_up = (*(volatile uint32_t *)err & kErrLookback) != 0;
+            if (give_up) {
                 if (lane == 0)
                     set_err(err, kErrLookback);
                 break;
