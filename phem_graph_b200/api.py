@@ -21,6 +21,8 @@ def as_edges(E) -> np.ndarray:
     """{u, v, w} records as an (m, 3) uint32 C array."""
     if isinstance(E, np.ndarray) and E.dtype == EDGE_DTYPE:
         return E.view(np.uint32).reshape(-1, 3)
+    if isinstance(E, np.ndarray) and E.dtype.itemsize == 4 and E.dtype.kind in "iu" and E.flags["C_CONTIGUOUS"]:
+        return E.view(np.uint32).reshape(-1, 3)  # same bits, no copy (keeps pinned memory pinned)
     E = np.ascontiguousarray(E, np.uint32)
     return E.reshape(-1, 3)
 
@@ -145,14 +147,18 @@ class Context:
         return ms.value
 
     # ------------------------------------------------------------ MSF
-    def msf_solve(self, edges, n: int, want_edges: bool = True) -> MSFResult:
-        """Unique MSF under (w, id) of {u, v, w} records; see phem_msf_solve."""
+    def msf_solve(self, edges, n: int, want_edges: bool = True, out=None) -> MSFResult:
+        """Unique MSF under (w, id) of {u, v, w} records; see phem_msf_solve.
+        `out` may supply the (>= n - 1, 3) result buffer (e.g. pinned memory)."""
         if isinstance(edges, np.ndarray):
             edges = as_edges(edges)
             m = len(edges)
-        else:  # torch tensor of shape (m, 3) uint32/int32 on the device
+        else:  # torch tensor of shape (m, 3) uint32/int32, host or device
             m = int(edges.shape[0])
-        out = np.empty((max(n - 1, 1), 3), np.uint32) if want_edges else None
+        if out is not None:
+            out = as_edges(out) if isinstance(out, np.ndarray) else out
+        elif want_edges:
+            out = np.empty((max(n - 1, 1), 3), np.uint32)
         cnt, tot = C.c_uint64(), C.c_uint64()
         st = MSFStats()
         check(lib().phem_msf_solve(self._h, ptr(edges), m, n, ptr(out), C.byref(cnt), C.byref(tot), C.byref(st)),
