@@ -102,6 +102,16 @@ phem_status phem_context_set_profiling(phem_context *ctx, int on);
 phem_status phem_context_profile(phem_context *ctx, phem_kernel_profile *out, uint32_t max, uint32_t *count);
 phem_status phem_context_profile_reset(phem_context *ctx);
 
+/* Tuning knobs (defaults suit B200; the autotuner may change them):
+ *   "msf.light_per_vertex"  light edges per vertex taken by the MSF filter
+ *                           before the heavy pass; 0 disables the filter   [2.0]
+ *   "msf.filter_min_ratio"  filter only when m >= ratio * light edges      [2.0]
+ *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
+ *   "msf.next_batch"        rounds queued per later check                 [4]
+ * None of them changes a result. */
+phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double value);
+phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *value);
+
 /* Releases the context's device workspace (it grows on demand otherwise). */
 phem_status phem_context_trim(phem_context *ctx);
 
@@ -119,12 +129,15 @@ typedef struct phem_cc_stats {
 } phem_cc_stats;
 
 typedef struct phem_msf_stats {
-    uint32_t rounds;                     /* rounds that hooked at least one component */
-    uint32_t pad;
-    uint64_t m_r[PHEM_MAX_ROUNDS];       /* live edges entering round r */
-    uint64_t n_r[PHEM_MAX_ROUNDS];       /* components with a live edge entering round r */
+    uint32_t rounds;                     /* Boruvka rounds run (light phase + heavy phase) */
+    uint32_t light_rounds;               /* rounds of the light phase; round light_rounds
+                                            is the pass that filters the heavy edges */
+    uint64_t m_r[PHEM_MAX_ROUNDS];       /* live edges found by round r's edge pass */
+    uint64_t n_r[PHEM_MAX_ROUNDS];       /* components that chose an edge in round r */
     uint64_t msf_edges;                  /* = n - components */
     uint64_t total_weight;               /* uint64 sum of MSF weights */
+    uint64_t threshold;                  /* light edge <=> (w << 32 | id) < threshold
+                                            (packed CC edges: id < threshold); all ones = no filter */
     float device_ms;                     /* GPU time of the solve, CUDA events on the stream */
 } phem_msf_stats;
 

@@ -43,9 +43,10 @@ class CCStats(C.Structure):
 
 
 class MSFStats(C.Structure):
-    _fields_ = [("rounds", C.c_uint32), ("pad", C.c_uint32),
+    _fields_ = [("rounds", C.c_uint32), ("light_rounds", C.c_uint32),
                 ("m_r", C.c_uint64 * PHEM_MAX_ROUNDS), ("n_r", C.c_uint64 * PHEM_MAX_ROUNDS),
-                ("msf_edges", C.c_uint64), ("total_weight", C.c_uint64), ("device_ms", C.c_float)]
+                ("msf_edges", C.c_uint64), ("total_weight", C.c_uint64), ("threshold", C.c_uint64),
+                ("device_ms", C.c_float)]
 
 
 class KernelProfile(C.Structure):
@@ -67,6 +68,8 @@ SIGNATURES = {
     "phem_context_stream": (_VP, [_VP]),
     "phem_context_set_timeout_ms": (C.c_int, [_VP, C.c_uint32]),
     "phem_context_trim": (C.c_int, [_VP]),
+    "phem_context_set_tuning": (C.c_int, [_VP, C.c_char_p, C.c_double]),
+    "phem_context_get_tuning": (C.c_int, [_VP, C.c_char_p, C.POINTER(C.c_double)]),
     "phem_context_set_profiling": (C.c_int, [_VP, C.c_int]),
     "phem_context_profile": (C.c_int, [_VP, C.POINTER(KernelProfile), C.c_uint32, C.POINTER(C.c_uint32)]),
     "phem_context_profile_reset": (C.c_int, [_VP]),

@@ -46,6 +46,8 @@ class MSFResult:
     m_r: list = field(default_factory=list)
     n_r: list = field(default_factory=list)
     device_ms: float = 0.0
+    light_rounds: int = 0
+    threshold: int = 0
 
 
 class Context:
@@ -87,6 +89,15 @@ class Context:
 
     def trim(self) -> None:
         check(lib().phem_context_trim(self._h), "phem_context_trim")
+
+    def set_tuning(self, key: str, value: float) -> None:
+        """Sets a tuning knob (see phem_context_set_tuning); results never depend on it."""
+        check(lib().phem_context_set_tuning(self._h, key.encode(), float(value)), "phem_context_set_tuning")
+
+    def get_tuning(self, key: str) -> float:
+        v = C.c_double()
+        check(lib().phem_context_get_tuning(self._h, key.encode(), C.byref(v)), "phem_context_get_tuning")
+        return v.value
 
     def set_profiling(self, on: bool) -> None:
         """Brackets every kernel launch with CUDA events (per-kernel durations)."""
@@ -164,9 +175,7 @@ class Context:
         check(lib().phem_msf_solve(self._h, ptr(edges), m, n, ptr(out), C.byref(cnt), C.byref(tot), C.byref(st)),
               "phem_msf_solve")
         k = int(cnt.value)
-        r = int(st.rounds)
-        return MSFResult(out[:k] if out is not None else None, k, int(tot.value), r,
-                         [int(x) for x in st.m_r[:r]], [int(x) for x in st.n_r[:r]], float(st.device_ms))
+        return _msf_result(out[:k] if out is not None else None, k, int(tot.value), st)
 
     def msf_solve_device(self, d_edges, m: int, n: int, d_msf=None, d_count_total=None) -> MSFResult:
         """Device-resident solve (torch tensors); counts stay on the device
@@ -174,9 +183,7 @@ class Context:
         st = MSFStats()
         check(lib().phem_msf_solve_device(self._h, ptr(d_edges), m, n, ptr(d_msf), ptr(d_count_total),
                                           C.byref(st)), "phem_msf_solve_device")
-        r = int(st.rounds)
-        return MSFResult(None, int(st.msf_edges), int(st.total_weight), r, [int(x) for x in st.m_r[:r]],
-                         [int(x) for x in st.n_r[:r]], float(st.device_ms))
+        return _msf_result(None, int(st.msf_edges), int(st.total_weight), st)
 
     def msf_solve_csr(self, offsets, cols, n: int, weights, m_upper: int) -> MSFResult:
         out = np.empty((max(n - 1, 1), 3), np.uint32)
@@ -185,9 +192,7 @@ class Context:
         check(lib().phem_msf_solve_csr(self._h, ptr(offsets), ptr(cols), n, ptr(weights), m_upper, ptr(out),
                                        C.byref(cnt), C.byref(tot), C.byref(st)), "phem_msf_solve_csr")
         k = int(cnt.value)
-        r = int(st.rounds)
-        return MSFResult(out[:k], k, int(tot.value), r, [int(x) for x in st.m_r[:r]],
-                         [int(x) for x in st.n_r[:r]], float(st.device_ms))
+        return _msf_result(out[:k], k, int(tot.value), st)
 
     def csr_to_coo(self, offsets, cols, n: int) -> np.ndarray:
         nnz = int(offsets[n])
@@ -195,6 +200,12 @@ class Context:
         k = C.c_int64()
         check(lib().phem_csr_to_coo(self._h, ptr(offsets), ptr(cols), n, ptr(out), C.byref(k)), "phem_csr_to_coo")
         return out[: k.value]
+
+
+def _msf_result(edges, count: int, total: int, st) -> MSFResult:
+    r = min(int(st.rounds), len(st.m_r))
+    return MSFResult(edges, count, total, int(st.rounds), [int(x) for x in st.m_r[:r]], [int(x) for x in st.n_r[:r]],
+                     float(st.device_ms), int(st.light_rounds), int(st.threshold))
 
 
 def forest_set(forest: np.ndarray) -> np.ndarray:

@@ -70,7 +70,7 @@ struct Timed {
 }  // namespace
 
 const char *const kKernelNames[kKernelCount] = {
-    "msf_init", "msf_round0", "msf_edge_pass", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
+    "msf_init", "msf_select", "msf_edge_pass", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
     "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "csr_pack"};
 
 static cudaEvent_t pool_get(phem_context *ctx)
@@ -449,6 +449,52 @@ phem_status phem_context_profile_reset(phem_context *ctx)
     return PHEM_OK;
 }
 
+phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double value)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (!key) {
+        set_error("set_tuning: null key");
+        return PHEM_ERR_INVALID;
+    }
+    const std::string k(key);
+    if (k == "msf.light_per_vertex" && value >= 0 && value < 1e6) {
+        ctx->tune_light_per_vertex = value;
+    } else if (k == "msf.filter_min_ratio" && value >= 1.0 && value < 1e6) {
+        ctx->tune_filter_min_ratio = value;
+    } else if (k == "msf.first_batch" && value >= 1 && value <= PHEM_MAX_ROUNDS) {
+        ctx->tune_first_batch = (int)value;
+    } else if (k == "msf.next_batch" && value >= 1 && value <= PHEM_MAX_ROUNDS) {
+        ctx->tune_next_batch = (int)value;
+    } else {
+        set_error("set_tuning: unknown key or value out of range: %s = %g", key, value);
+        return PHEM_ERR_INVALID;
+    }
+    return PHEM_OK;
+}
+
+phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *value)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (!key || !value) {
+        set_error("get_tuning: null argument");
+        return PHEM_ERR_INVALID;
+    }
+    const std::string k(key);
+    if (k == "msf.light_per_vertex")
+        *value = ctx->tune_light_per_vertex;
+    else if (k == "msf.filter_min_ratio")
+        *value = ctx->tune_filter_min_ratio;
+    else if (k == "msf.first_batch")
+        *value = ctx->tune_first_batch;
+    else if (k == "msf.next_batch")
+        *value = ctx->tune_next_batch;
+    else {
+        set_error("get_tuning: unknown key %s", key);
+        return PHEM_ERR_INVALID;
+    }
+    return PHEM_OK;
+}
+
 phem_status phem_context_trim(phem_context *ctx)
 {
     PHEM_TRY(check_ctx(ctx));
@@ -700,6 +746,8 @@ static phem_status msf_common(phem_context *ctx, const phem_edge *edges, uint64_
             stats->m_r[r] = h.m_r[r];
             stats->n_r[r] = h.n_r[r];
         }
+        stats->light_rounds = h.light_rounds;
+        stats->threshold = h.threshold;
         stats->msf_edges = h.msf_count;
         stats->total_weight = h.msf_total;
         stats->device_ms = ms;

@@ -35,7 +35,12 @@ struct Ctl {
     uint32_t err;
     uint32_t round;                                  // device-side round counter
     uint32_t go;                                     // 1 while another round is needed
+    uint32_t phase;                                  // 0: light edges, 1: heavy edges
+    uint32_t src;                                    // input of this round's edge pass (kSrc*)
+    uint32_t cand_all;                               // this round's candidates are all n vertices
+    uint32_t light_rounds;                           // rounds spent in the light phase
     uint32_t pad0;
+    unsigned long long threshold;                    // light edge <=> key < threshold
     unsigned long long m_r[PHEM_MAX_ROUNDS + 1];     // live edges entering round r
     unsigned long long n_r[PHEM_MAX_ROUNDS + 1];     // components with a live edge in round r
     uint32_t roots[PHEM_MAX_ROUNDS + 2];             // |candidate roots| entering round r
@@ -45,6 +50,13 @@ struct Ctl {
     unsigned long long msf_count;
     unsigned long long msf_total;
     unsigned long long misc[8];
+};
+
+// Input of an edge pass.
+enum : uint32_t {
+    kSrcLight = 0,  // the caller's edges, keeping key < threshold; endpoints are their own roots
+    kSrcList = 1,   // the previous round's survivor records
+    kSrcHeavy = 2,  // the caller's edges, keeping key >= threshold; endpoints relabelled by parent[]
 };
 
 // ---------------------------------------------------------------- memory helpers

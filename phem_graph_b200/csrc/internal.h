@@ -14,7 +14,7 @@
 namespace phem {
 // Kernels the library launches; the profile reports them by these names.
 enum KernelId : int {
-    kKInit = 0, kKRound0, kKEdgePass, kKHook, kKCompress, kKAdvance, kKGather,
+    kKInit = 0, kKSelect, kKEdgePass, kKHook, kKCompress, kKAdvance, kKGather,
     kKCcInit, kKCcUnite, kKCcMerge, kKCcLabel, kKMinid, kKCcCount, kKCsrCoo, kKPack,
     kKernelCount
 };
@@ -42,8 +42,12 @@ struct phem_context {
     uint32_t timeout_ms = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     int edge_pass_blocks = 0;          // persistent grid sizes, from the occupancy API
-    int round0_blocks = 0;
     int gather_blocks = 0;
+    // tuning knobs (phem_context_set_tuning)
+    double tune_light_per_vertex = 2.0;  // light edges per vertex in the MSF filter (0: no filter)
+    double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
+    int tune_first_batch = 8;            // Boruvka rounds queued before the first host check
+    int tune_next_batch = 4;             // rounds queued per later check
     // launch accounting and optional per-kernel CUDA-event timing
     uint64_t launches[phem::kKernelCount] = {};
     double kernel_ms[phem::kKernelCount] = {};

@@ -1,30 +1,40 @@
-// msf.cu -- Boruvka minimum spanning forest on sm_100a.
+// msf.cu -- minimum spanning forest on sm_100a: Boruvka rounds behind a
+// light/heavy edge filter.
 //
-// Same arithmetic as the reference's device_boruvka (MST/src/kernels.cu:507-689):
+// Arithmetic is the reference's device_boruvka (MST/src/kernels.cu:507-689):
 // per round every component takes its minimum (weight, edge id) edge, a
 // mutual pair keeps the lower id as root and every other chooser hooks onto
 // the far component (new_grafting_edges, :73-134), hooks are jumped to roots
 // (new_shortcutting_step, :254-271) and edges inside a component are dropped
-// (relabelling_step / filtering_step / remove_if, :273-321, :641-649).
+// (relabelling_step / filtering_step / remove_if, :273-321, :641-649).  The
+// order (weight, edge id) is strict, so the forest is the unique MSF that the
+// reference's PBBS mst() (MST/src/utils.cu:794-841) returns.
 //
-// Layout and kernels are B200-first rather than a translation:
-//   * round 0 reads the 12-byte {u,v,w} input with 128-bit streaming loads and
-//     reduces (w << 32 | id) keys per endpoint inside each warp before one
-//     guarded 64-bit atomicMin per distinct endpoint;
-//   * rounds >= 1 run ONE streaming pass per round over the live edges: it
-//     relabels both endpoints to their roots, drops internal edges, writes the
-//     survivors as 16-byte {root_u, root_v, w, id} records with a stable
-//     single-pass compaction (decoupled look-back) and offers each survivor's
-//     key to both roots in the same pass.  Because the compaction is stable the
-//     survivor's position orders like its id, so the key carries the position
-//     and the hook step finds the record directly;
-//   * the vertex steps (hook, pointer jumping) only visit the components that
-//     were roots at the start of the round, kept in a compacted list;
-//   * MSF membership is a bitmap over edge ids; one final ordered gather writes
-//     the MSF records ascending by id with the uint64 total.
-// Every kernel reads the round number and the continue flag from the device
-// control block, so the host can queue rounds ahead without reading anything
-// back; a round queued after convergence exits at once.
+// Order of work (B200 design, not a translation):
+//   1. A one-CTA kernel picks a weight threshold from a stratified sample of
+//      the input so that about `light_per_vertex * n` edges are light.  This is
+//      the filtering step of PBBS mst() (approximate k-th smallest, :805-813),
+//      done on the device.
+//   2. Light phase.  Round 0 streams the input once with 128-bit loads and
+//      keeps only light edges; later rounds stream the (small) survivor list.
+//      Each round is ONE pass: relabel both endpoints to their roots, drop
+//      internal edges, write survivors as 16-byte {root_u, root_v, w, id}
+//      records with a stable single-pass compaction (decoupled look-back), and
+//      offer each survivor's key to both roots in the same pass.  Because the
+//      compaction is stable a survivor's position orders like its id, so keys
+//      carry (w, position) and the hook step reads the record directly.
+//   3. When no light edge is left the parents of all vertices are compressed
+//      and the input is streamed a second time keeping heavy edges whose
+//      endpoints lie in different components (PBBS's second filter, :819-823);
+//      Boruvka continues on those survivors.
+//   An edge that is heavy and internal after the light phase closes a cycle of
+//   lighter edges, so it is in no MSF: the filter changes the work, not the
+//   result.
+// MSF membership is a bitmap over edge ids; one ordered gather writes the MSF
+// records ascending by id with the uint64 total.  Every kernel reads the
+// round, phase and continue flag from the device control block, so rounds are
+// queued ahead without host round trips; a round queued after convergence
+// exits at once.
 #include <algorithm>
 #include <cstring>
 
@@ -50,8 +60,8 @@ struct RoundArgs {
 
 // ---- input record access --------------------------------------------------
 
-// Four consecutive input records starting at index `base` (a multiple of 4).
-// ok[j] is false past the end of the input.
+// Four consecutive input records starting at index `base` (a multiple of 4),
+// read with 128-bit evict-first loads.  ok[j] is false past the end.
 template <int KIND>
 __device__ __forceinline__ void load4_e0(const void *e0, uint64_t base, uint64_t m, uint32_t (&u)[4],
                                          uint32_t (&v)[4], uint32_t (&w)[4], bool (&ok)[4])
@@ -111,18 +121,44 @@ __device__ __forceinline__ bool e0_live(uint32_t u, uint32_t v)
     return KIND == kKindMsf ? (u != v) : (u < v);
 }
 
+// Key that decides light/heavy: (w, id) for weighted edges, id for packed CC
+// edges (the canonical forest orders edges by index alone).
 template <int KIND>
-__device__ __forceinline__ void e0_endpoints(const void *e0, uint32_t id, uint32_t &u, uint32_t &v)
+__device__ __forceinline__ unsigned long long e0_key(uint32_t w, uint64_t id)
 {
-    if (KIND == kKindMsf) {
-        const uint32_t *p = reinterpret_cast<const uint32_t *>(e0) + (uint64_t)id * 3;
-        u = __ldg(p);
-        v = __ldg(p + 1);
-    } else {
-        unsigned long long e = __ldg(reinterpret_cast<const unsigned long long *>(e0) + id);
-        u = (uint32_t)(e >> 32);
-        v = (uint32_t)e;
+    return KIND == kKindMsf ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
+}
+
+// Offers key k[j] to best[t[j]] for live slots j: equal targets among the four
+// are folded first, then every guard load is issued before any atomic, so the
+// four L2 round trips overlap.  The guard read may be stale but never below
+// the true minimum, so it only skips atomics that could not lower it.
+__device__ __forceinline__ void offer4(unsigned long long *best, const uint32_t (&t)[4],
+                                       const unsigned long long (&k)[4], const bool (&ok)[4])
+{
+    bool o[4];
+    unsigned long long kk[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        o[j] = ok[j];
+        kk[j] = k[j];
     }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int i = j + 1; i < 4; i++)
+            if (o[j] && o[i] && t[i] == t[j]) {
+                kk[j] = kk[i] < kk[j] ? kk[i] : kk[j];
+                o[i] = false;
+            }
+    unsigned long long g[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        g[j] = o[j] ? __ldcg(best + t[j]) : 0ull;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (o[j] && kk[j] < g[j])
+            atomicMin(best + t[j], kk[j]);
 }
 
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
@@ -141,9 +177,16 @@ __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x
     return t;  // valid in thread 0
 }
 
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
 // ---- kernels -----------------------------------------------------------------
 
-__global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a)
+__global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a, unsigned long long threshold)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.n; x += stride) {
@@ -153,52 +196,86 @@ __global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a)
             a.forest[x] = kForestEmpty;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        a.ctl->go = 1;
-        a.ctl->round = 0;
+        Ctl *c = a.ctl;
+        c->go = 1;
+        c->round = 0;
+        c->phase = 0;
+        c->src = kSrcLight;
+        c->cand_all = 1;
+        c->threshold = threshold;
     }
 }
 
-// Round 0: every vertex is its own component; best[x] = min key over incident
-// live edges, key = (w << 32 | input index).  Also counts m_0.
-template <int KIND>
-__global__ void __launch_bounds__(kBlock) round0_kernel(RoundArgs a)
+// Weight threshold from a stratified sample of kSample input weights: the
+// sample's `rank`-th smallest weight, found by a three-digit radix select in
+// shared memory (one CTA).  Light edges are those with w below it.
+constexpr int kSample = 8192;
+constexpr int kSelectThreads = 1024;
+
+__global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const uint32_t *e0, uint64_t m,
+                                                                          uint64_t k, Ctl *ctl)
 {
-    __shared__ unsigned long long s_red[kWarps];
-    const uint64_t groups = (a.m + 3) / 4;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    unsigned long long live = 0;
-    for (uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x; g0 < groups; g0 += stride) {
-        const uint64_t g = g0 + threadIdx.x;
-        uint32_t u[4], v[4], w[4];
-        bool ok[4];
-        if (g < groups) {
-            load4_e0<KIND>(a.e0, g * 4, a.m, u, v, w, ok);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                ok[j] = false;
-                u[j] = v[j] = w[j] = 0;
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            bool valid = ok[j] && e0_live<KIND>(u[j], v[j]);
-            if (valid && (u[j] >= a.n || v[j] >= a.n)) {
-                set_err(&a.ctl->err, kErrRange);
-                valid = false;
-            }
-            live += valid;
-            const uint64_t key = ((uint64_t)w[j] << 32) | (uint32_t)(g * 4 + j);
-            warp_min_to(a.best, u[j], key, valid);
-            warp_min_to(a.best, v[j], key, valid);
-        }
+    __shared__ uint32_t samp[kSample];
+    __shared__ uint32_t hist[2048];
+    __shared__ uint32_t s_prefix, s_rank;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < kSample; i += kSelectThreads) {
+        const uint64_t lo = (uint64_t)i * m / kSample, hi = (uint64_t)(i + 1) * m / kSample;
+        const uint64_t pos = hi > lo ? lo + mix64(0x5EED0000ull + i) % (hi - lo) : lo;
+        samp[i] = e0[pos * 3 + 2];
     }
-    const unsigned long long t = block_sum_u64(live, s_red);
-    if (threadIdx.x == 0 && t)
-        atomicAdd(&a.ctl->m_r[0], t);
+    if (tid == 0) {
+        s_prefix = 0;
+        s_rank = (uint32_t)(k * kSample / m);
+    }
+    const int shifts[3] = {21, 10, 0}, bits[3] = {11, 11, 10};
+    for (int d = 0; d < 3; d++) {
+        const int sh = shifts[d], nb = bits[d], hsh = sh + nb;
+        for (int i = tid; i < 2048; i += kSelectThreads)
+            hist[i] = 0;
+        __syncthreads();
+        const uint64_t want_hi = (uint64_t)s_prefix >> hsh;
+        for (int i = tid; i < kSample; i += kSelectThreads) {
+            const uint32_t x = samp[i];
+            if (((uint64_t)x >> hsh) == want_hi)
+                atomicAdd(&hist[(x >> sh) & ((1u << nb) - 1)], 1u);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            // lane l owns bins [64 l, 64 l + 64)
+            uint32_t sum = 0;
+            for (int b = 0; b < 64; b++)
+                sum += hist[tid * 64 + b];
+            uint32_t incl = sum;
+#pragma unroll
+            for (int s = 1; s < 32; s <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, incl, s);
+                if (tid >= s)
+                    incl += y;
+            }
+            const uint32_t excl = incl - sum, rank = s_rank;
+            const bool mine = rank >= excl && rank < incl;
+            if (mine) {
+                uint32_t c = excl;
+                for (int b = 0; b < 64; b++) {
+                    const uint32_t h = hist[tid * 64 + b];
+                    if (rank < c + h) {
+                        s_prefix |= (uint32_t)(tid * 64 + b) << sh;
+                        s_rank = rank - c;
+                        break;
+                    }
+                    c += h;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0)
+        ctl->threshold = (unsigned long long)s_prefix << 32;
 }
 
-// Rounds >= 1: relabel + filter + stable compaction + per-root minimum, one pass.
+// One Boruvka round's edge pass: relabel + filter + stable compaction +
+// per-root minimum.
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) edge_pass_kernel(RoundArgs a)
 {
@@ -208,7 +285,9 @@ __global__ void __launch_bounds__(kBlock) edge_pass_kernel(RoundArgs a)
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
-    const bool from_e0 = (r == 1);
+    const uint32_t src = *(volatile uint32_t *)&ctl->src;
+    const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
+    const bool from_e0 = src != kSrcList;
     const uint64_t count = from_e0 ? a.m : ctl->m_r[r - 1];
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
     uint4 *out = (r & 1) ? a.wl1 : a.wl0;       // WL[r & 1]
@@ -230,7 +309,14 @@ __global__ void __launch_bounds__(kBlock) edge_pass_kernel(RoundArgs a)
             load4_e0<KIND>(a.e0, base, count, u, v, w, ok);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                keep[j] = ok[j] && e0_live<KIND>(u[j], v[j]) && u[j] < a.n && v[j] < a.n;
+                bool live = ok[j] && e0_live<KIND>(u[j], v[j]);
+                if (live && (u[j] >= a.n || v[j] >= a.n)) {
+                    if (src == kSrcLight)
+                        set_err(&ctl->err, kErrRange);
+                    live = false;
+                }
+                const bool light = e0_key<KIND>(w[j], base + j) < thr;
+                keep[j] = live && (src == kSrcLight ? light : !light);
                 ra[j] = u[j];
                 rb[j] = v[j];
                 id[j] = (uint32_t)(base + j);
@@ -250,11 +336,11 @@ __global__ void __launch_bounds__(kBlock) edge_pass_kernel(RoundArgs a)
         uint32_t c = 0;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            if (keep[j]) {
+            if (keep[j] && src != kSrcLight) {  // light round 0: every vertex is its own root
                 ra[j] = __ldg(a.parent + ra[j]);
                 rb[j] = __ldg(a.parent + rb[j]);
-                keep[j] = ra[j] != rb[j];
             }
+            keep[j] = keep[j] && ra[j] != rb[j];
             c += keep[j];
         }
         uint32_t total;
@@ -269,15 +355,16 @@ __global__ void __launch_bounds__(kBlock) edge_pass_kernel(RoundArgs a)
         }
         __syncthreads();
         uint32_t pos = s_base + off;
+        unsigned long long key[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
+            key[j] = ((unsigned long long)w[j] << 32) | pos;
             if (keep[j])
                 out[pos] = make_uint4(ra[j], rb[j], w[j], id[j]);
-            const uint64_t key = ((uint64_t)w[j] << 32) | pos;
-            warp_min_to(a.best, ra[j], key, keep[j]);
-            warp_min_to(a.best, rb[j], key, keep[j]);
             pos += keep[j];
         }
+        offer4(a.best, ra, key, keep);
+        offer4(a.best, rb, key, keep);
         __syncthreads();
     }
 }
@@ -291,30 +378,22 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
-    const uint32_t count = (r == 0) ? a.n : ctl->roots[r];
+    const bool all = *(volatile uint32_t *)&ctl->cand_all;
+    const uint32_t count = all ? a.n : ctl->roots[r];
     const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
     const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < count; i0 += stride) {
         const uint32_t i = i0 + threadIdx.x;
         const bool in = i < count;
-        const uint32_t x = in ? (r == 0 ? i : cand[i]) : 0;
+        const uint32_t x = in ? (all ? i : cand[i]) : 0;
         const unsigned long long bk = in ? a.best[x] : kKeyNone;
         const bool active = bk != kKeyNone;
         warp_count(&ctl->n_r[r], active);
         if (!active)
             continue;
-        const uint32_t pos = (uint32_t)bk;
-        uint32_t ea, eb, id;
-        if (r == 0) {
-            e0_endpoints<KIND>(a.e0, pos, ea, eb);
-            id = pos;
-        } else {
-            const uint4 rec = wl[pos];
-            ea = rec.x;
-            eb = rec.y;
-            id = rec.w;
-        }
+        const uint4 rec = wl[(uint32_t)bk];
+        const uint32_t ea = rec.x, eb = rec.y, id = rec.w;
         if (ea != x && eb != x) {
             set_err(&ctl->err, kErrChase);
             continue;
@@ -330,23 +409,27 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
     }
 }
 
-// Pointer jumping over this round's components; roots that remain are
-// collected (in any order) as the next round's candidates.  Also resets best.
+// Pointer jumping.  Normally over this round's components only: roots that
+// remain are collected as the next round's candidates and best is reset.  In
+// the round where the light phase runs dry every vertex is compressed to its
+// root instead, so the heavy pass can relabel original endpoints in one hop.
 __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
 {
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
-    const uint32_t count = (r == 0) ? a.n : ctl->roots[r];
+    const bool all = *(volatile uint32_t *)&ctl->cand_all;
+    const bool full = *(volatile uint32_t *)&ctl->phase == 0 && ctl->m_r[r] == 0;
+    const uint32_t count = (all || full) ? a.n : ctl->roots[r];
     const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
     uint32_t *next = (r & 1) ? a.cand0 : a.cand1;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < count; i0 += stride) {
         const uint32_t i = i0 + threadIdx.x;
         const bool in = i < count;
-        const uint32_t x = in ? (r == 0 ? i : cand[i]) : 0;
-        const bool active = in && a.best[x] != kKeyNone;
+        const uint32_t x = in ? ((all || full) ? i : cand[i]) : 0;
+        const bool active = in && (full || a.best[x] != kKeyNone);
         bool stays = false;
         if (active) {
             uint32_t y = a.parent[x];
@@ -361,9 +444,12 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
                     break;
                 }
             }
-            a.parent[x] = y;
-            a.best[x] = kKeyNone;
-            stays = (y == x);
+            if (a.parent[x] != y)
+                a.parent[x] = y;
+            if (!full) {
+                a.best[x] = kKeyNone;
+                stays = (y == x);
+            }
         }
         const unsigned b = __ballot_sync(0xffffffffu, stays);
         uint32_t slot = 0;
@@ -375,13 +461,28 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
     }
 }
 
-// Ends a round: another one is needed while this round still had live edges.
+// Ends a round.  Live edges left -> another round on the survivor list.  No
+// light edge left -> switch to the heavy pass (if there is a threshold).  No
+// heavy edge left -> done.
 __global__ void advance_kernel(Ctl *ctl)
 {
     if (!ctl->go)
         return;
     const uint32_t r = ctl->round;
-    bool again = ctl->m_r[r] > 0;
+    bool again;
+    if (ctl->m_r[r] > 0) {
+        ctl->src = kSrcList;
+        ctl->cand_all = 0;
+        again = true;
+    } else if (ctl->phase == 0) {
+        ctl->phase = 1;
+        ctl->light_rounds = r + 1;
+        ctl->src = kSrcHeavy;
+        ctl->cand_all = 1;
+        again = ctl->threshold != kKeyNone;
+    } else {
+        again = false;
+    }
     if (again && r + 1 >= PHEM_MAX_ROUNDS) {
         ctl->err |= kErrRounds;
         again = false;
@@ -515,61 +616,48 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
         ctx->edge_pass_blocks = ctx->sm_count * std::max(1, per_sm);
         PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
         ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
-        PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, round0_kernel<KIND>, kBlock, 0));
-        ctx->round0_blocks = ctx->sm_count * std::max(1, per_sm);
     }
     const RoundArgs a = make_args(ctx, plan);
+    // light/heavy split: about light_per_vertex * n light edges, and only when
+    // the input is at least filter_min_ratio times that large
+    const double lpv = ctx->tune_light_per_vertex;
+    const uint64_t k = (uint64_t)(lpv * (double)plan.n);
+    const bool filter = lpv > 0 && plan.m > 0 && (double)plan.m >= ctx->tune_filter_min_ratio * (double)k;
+    unsigned long long thr = kKeyNone;
+    if (filter && KIND == kKindPacked)
+        thr = k;  // canonical forest: the first k edges by index are light
     PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), s));
     PHEM_CUDA_TRY(cudaMemsetAsync(plan.bitmap, 0, ((plan.m + 31) / 32) * sizeof(uint32_t), s));
     {
-        KernelScope k(ctx, kKInit);
-        init_kernel<<<vertex_blocks(ctx, plan.n), kBlock, 0, s>>>(a);
+        KernelScope ks(ctx, kKInit);
+        init_kernel<<<vertex_blocks(ctx, plan.n), kBlock, 0, s>>>(a, thr);
     }
-    const uint64_t groups = (plan.m + 3) / 4;
-    const int r0_blocks = (int)std::max<uint64_t>(
-        1, std::min<uint64_t>((groups + kBlock - 1) / kBlock, (uint64_t)ctx->round0_blocks));
-    {
-        KernelScope k(ctx, kKRound0);
-        round0_kernel<KIND><<<r0_blocks, kBlock, 0, s>>>(a);
-    }
-    const int vb = vertex_blocks(ctx, plan.n);
-    {
-        KernelScope k(ctx, kKHook);
-        hook_kernel<KIND><<<vb, kBlock, 0, s>>>(a);
-    }
-    {
-        KernelScope k(ctx, kKCompress);
-        compress_kernel<<<vb, kBlock, 0, s>>>(a);
-    }
-    {
-        KernelScope k(ctx, kKAdvance);
-        advance_kernel<<<1, 1, 0, s>>>(a.ctl);
+    if (filter && KIND == kKindMsf) {
+        KernelScope ks(ctx, kKSelect);
+        select_threshold_kernel<<<1, kSelectThreads, 0, s>>>(static_cast<const uint32_t *>(plan.e0), plan.m, k,
+                                                             ctx->ctl);
     }
     PHEM_CUDA_TRY(cudaGetLastError());
     // Rounds are queued in batches; the host reads the continue flag between
     // batches.  Rounds queued after convergence return immediately.
-    int queued = 1;
-    int batch = 3;
+    int queued = 0;
+    int batch = ctx->tune_first_batch;
     while (queued < PHEM_MAX_ROUNDS) {
-        for (int k = 0; k < batch && queued < PHEM_MAX_ROUNDS; k++, queued++)
+        for (int b = 0; b < batch && queued < PHEM_MAX_ROUNDS; b++, queued++)
             PHEM_TRY(queue_round<KIND>(ctx, a));
-        PHEM_CUDA_TRY(cudaMemcpyAsync(&ctx->h_ctl->go, &ctx->ctl->go, sizeof(uint32_t) * 2,
-                                      cudaMemcpyDeviceToHost, s));
+        PHEM_CUDA_TRY(cudaMemcpyAsync(&ctx->h_ctl->go, &ctx->ctl->go, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         PHEM_TRY(stream_wait(ctx));
         if (!*(volatile uint32_t *)&ctx->h_ctl->go)
             break;
-        batch = 2;
+        batch = ctx->tune_next_batch;
     }
     PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     PHEM_TRY(stream_wait(ctx));
     const Ctl &h = *ctx->h_ctl;
     if (h.go)
         return ctl_status(h.err | kErrRounds, "msf");
-    uint32_t rounds = 0;
-    while (rounds < PHEM_MAX_ROUNDS && h.m_r[rounds] > 0)
-        rounds++;
     if (rounds_out)
-        *rounds_out = rounds;
+        *rounds_out = h.round;
     return ctl_status(h.err, "msf");
 }
 

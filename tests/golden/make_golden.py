@@ -84,9 +84,31 @@ def _cc_child(name: str) -> None:
     np.savez(HERE / f"_tmp_{name}.npz", parent=parent, sptree=sptree)
 
 
+def rmat22_rounds() -> None:
+    """Per-round live counts of the MSF benchmark workload (R-MAT scale 22, edge
+    factor 16, seed 22) from the CPU Boruvka restatement, with the MSF size and
+    total pinned by the reference's PBBS mst().  bench.py reads this file for
+    the algorithmic byte model of a solve."""
+    import oracle
+    from phem_graph_b200 import gen
+    g = gen.rmat_graph(22, 16, seed=22)
+    E = g.msf_edges()
+    flags, cnt, tot, m_r, n_r = oracle.msf_boruvka(E, g.n)
+    ids = oracle.ref_pbbs_mst(E)
+    assert len(ids) == cnt and int(E[ids, 2].astype(np.uint64).sum()) == tot
+    out = {"workload": "msf_rmat22_ef16", "n": g.n, "m": g.m, "seed": 22, "weight_seed": 1022,
+           "m_r": [int(x) for x in m_r], "n_r": [int(x) for x in n_r], "msf_edges": cnt, "total_weight": tot,
+           "source": "oracle/phem_oracle.c oracle_msf_boruvka; count and total equal PBBS mst()"}
+    (HERE / "rmat22_boruvka_rounds.json").write_text(json.dumps(out, indent=1) + "\n")
+    print(json.dumps(out))
+
+
 def main() -> None:
     if len(sys.argv) == 3 and sys.argv[1] == "--cc-child":
         _cc_child(sys.argv[2])
+        return
+    if len(sys.argv) == 2 and sys.argv[1] == "--rmat22":
+        rmat22_rounds()
         return
     import oracle
     if not oracle.ref_available():

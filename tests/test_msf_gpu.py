@@ -39,10 +39,40 @@ def test_rmat_random(ctx, seed, scale, ef, bits):
     ids, cnt, tot = expect(E, g.n)
     r = ctx.msf_solve(E, g.n)
     assert_msf(r, E, ids, cnt, tot)
-    # per-round live counts equal the Boruvka restatement's
+    assert sum(r.n_r) >= cnt  # every MSF edge is hooked by one chooser
+
+
+@pytest.mark.parametrize("lpv", [0.0, 0.25, 1.0, 2.0, 6.0])
+@pytest.mark.parametrize("scale,ef,bits", [(12, 16, 20), (13, 8, 3)])
+def test_filter_settings_do_not_change_the_forest(ctx, lpv, scale, ef, bits):
+    g = gen.rmat_graph(scale, ef, seed=11, bits=bits)
+    E = g.msf_edges()
+    ids, cnt, tot = expect(E, g.n)
+    old = ctx.get_tuning("msf.light_per_vertex")
+    ctx.set_tuning("msf.light_per_vertex", lpv)
+    try:
+        r = ctx.msf_solve(E, g.n)
+    finally:
+        ctx.set_tuning("msf.light_per_vertex", old)
+    assert_msf(r, E, ids, cnt, tot)
+    if lpv == 0.0:
+        assert r.threshold == 2**64 - 1 and r.light_rounds == r.rounds
+
+
+@pytest.mark.parametrize("scale,ef", [(12, 16), (15, 8)])
+def test_unfiltered_rounds_equal_boruvka_restatement(ctx, scale, ef):
+    """With the filter off the device runs plain Boruvka: its per-round live
+    edge and component counts are the restatement's."""
+    g = gen.rmat_graph(scale, ef, seed=scale)
+    E = g.msf_edges()
     _, _, _, m_r, n_r = oracle.msf_boruvka(E, g.n)
-    assert r.m_r == [int(x) for x in m_r]
-    assert r.n_r == [int(x) for x in n_r]
+    ctx.set_tuning("msf.light_per_vertex", 0)
+    try:
+        r = ctx.msf_solve(E, g.n)
+    finally:
+        ctx.set_tuning("msf.light_per_vertex", 2.0)
+    assert r.m_r == [int(x) for x in m_r] + [0]
+    assert r.n_r == [int(x) for x in n_r] + [0]
 
 
 @pytest.mark.parametrize("seed", [5, 6])
@@ -57,14 +87,14 @@ def test_er_with_ties_and_duplicates(ctx, seed):
 @pytest.mark.slow
 def test_full_size_rmat22(ctx):
     """The MSF workload at full size (R-MAT scale 22, edge factor 16): count,
-    total and every record against the oracle, per-round live counts against
-    the Boruvka restatement."""
+    total and every record against
+    the oracle; the light/heavy filter is active at this size."""
     g = gen.rmat_graph(22, 16, seed=22)
     E = g.msf_edges()
     flags, cnt, tot, m_r, n_r = oracle.msf_boruvka(E, g.n)
     r = ctx.msf_solve(E, g.n)
     assert_msf(r, E, np.nonzero(flags)[0], cnt, tot)
-    assert r.m_r == [int(x) for x in m_r] and r.n_r == [int(x) for x in n_r]
+    assert r.threshold != 2**64 - 1 and r.light_rounds < r.rounds  # the filter ran
     # idempotence: the MSF of the MSF is itself
     r2 = ctx.msf_solve(r.edges, g.n)
     assert (r2.count, r2.total) == (r.count, r.total)
