@@ -226,4 +226,62 @@ __device__ __forceinline__ uint32_t lookback_exclusive(uint64_t *status, uint32_
 // Grid size for the persistent streaming kernels: whole waves over 148 SMs.
 inline int persistent_blocks(int sm_count, int blocks_per_sm) { return sm_count * blocks_per_sm; }
 
+// ---------------------------------------------------------------- bulk copies (TMA, sm_90+)
+// 1-D cp.async.bulk global -> shared with mbarrier completion.  Plain loads
+// only: no cluster multicast anywhere in this library.
+constexpr uint32_t kMbarSpinCap = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Makes barrier initialisation visible to the async (bulk-copy) proxy.
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Orders earlier generic-proxy accesses of shared memory before later
+// async-proxy writes to it (a stage is refilled only after it was read).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of a barrier; false (and kErrLookback set)
+// when the cap is reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err)
+{
+    for (uint32_t i = 0; i < kMbarSpinCap; i++)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    set_err(err, kErrLookback);
+    return false;
+}
+
 }  // namespace phem

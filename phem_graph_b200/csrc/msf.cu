@@ -60,58 +60,6 @@ struct RoundArgs {
 
 // ---- input record access --------------------------------------------------
 
-// Four consecutive input records starting at index `base` (a multiple of 4),
-// read with 128-bit evict-first loads.  ok[j] is false past the end.
-template <int KIND>
-__device__ __forceinline__ void load4_e0(const void *e0, uint64_t base, uint64_t m, uint32_t (&u)[4],
-                                         uint32_t (&v)[4], uint32_t (&w)[4], bool (&ok)[4])
-{
-    if (KIND == kKindMsf) {
-        const uint32_t *p = reinterpret_cast<const uint32_t *>(e0) + base * 3;
-        if (base + 4 <= m) {
-            const uint4 *q = reinterpret_cast<const uint4 *>(p);
-            uint4 a = __ldcs(q), b = __ldcs(q + 1), c = __ldcs(q + 2);
-            u[0] = a.x; v[0] = a.y; w[0] = a.z;
-            u[1] = a.w; v[1] = b.x; w[1] = b.y;
-            u[2] = b.z; v[2] = b.w; w[2] = c.x;
-            u[3] = c.y; v[3] = c.z; w[3] = c.w;
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                ok[j] = true;
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                ok[j] = base + j < m;
-                u[j] = ok[j] ? __ldcs(p + 3 * j) : 0;
-                v[j] = ok[j] ? __ldcs(p + 3 * j + 1) : 0;
-                w[j] = ok[j] ? __ldcs(p + 3 * j + 2) : 0;
-            }
-        }
-    } else {
-        const unsigned long long *p = reinterpret_cast<const unsigned long long *>(e0) + base;
-        if (base + 4 <= m) {
-            const uint4 *q = reinterpret_cast<const uint4 *>(p);
-            uint4 a = __ldcs(q), b = __ldcs(q + 1);
-            v[0] = a.x; u[0] = a.y; v[1] = a.z; u[1] = a.w;
-            v[2] = b.x; u[2] = b.y; v[3] = b.z; u[3] = b.w;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                ok[j] = true;
-                w[j] = 0;
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                ok[j] = base + j < m;
-                unsigned long long e = ok[j] ? __ldcs(p + j) : 0ull;
-                u[j] = (uint32_t)(e >> 32);
-                v[j] = (uint32_t)e;
-                w[j] = 0;
-            }
-        }
-    }
-}
-
 // An input record takes part in the forest: self-loops never do; packed CC
 // edges follow union_find_gpu_COO and only count when u < v
 // (CC/ExternalSpanningTree.cu:82).
@@ -275,12 +223,30 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
 }
 
 // One Boruvka round's edge pass: relabel + filter + stable compaction +
-// per-root minimum.
+// per-root minimum, as a software pipeline.  Each persistent CTA owns up to
+// kStages tiles of kPipeTile records at a time: whole tiles arrive in shared
+// memory by 1-D bulk copies (cp.async.bulk, completion on an mbarrier) while
+// the CTA works on an earlier tile, so HBM streaming overlaps the relabel
+// gathers, the scan and the look-back.  Threads read a tile striped (record
+// j * kBlock + tid), which is conflict-free for 8, 12 and 16-byte records, and
+// the stable rank of a survivor is its warp-ballot prefix plus a 64-entry scan
+// of the (row, warp) counts.  Tiles are numbered by tickets taken in order
+// when a stage is refilled, so the decoupled look-back only ever waits on
+// tiles that running CTAs already own.
+constexpr int kPipeTile = 2048;
+constexpr int kPipeItems = kPipeTile / kBlock;  // 8 records per thread
+constexpr int kStages = 3;
+constexpr size_t kStageBytes = (size_t)kPipeTile * 16;  // sized for the widest record
+constexpr size_t kPipeSmem = kStages * kStageBytes;     // 96 KB
+
 template <int KIND>
-__global__ void __launch_bounds__(kBlock) edge_pass_kernel(RoundArgs a)
+__global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
 {
-    __shared__ uint32_t s_tile, s_base;
-    __shared__ uint32_t s_warp[kWarps + 1];
+    extern __shared__ __align__(128) unsigned char stage_mem[];
+    __shared__ uint64_t s_bar[kStages];
+    __shared__ uint32_t s_tile[kStages];
+    __shared__ uint32_t s_cnt[kPipeItems * kWarps];
+    __shared__ uint32_t s_base;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
@@ -291,80 +257,163 @@ __global__ void __launch_bounds__(kBlock) edge_pass_kernel(RoundArgs a)
     const uint64_t count = from_e0 ? a.m : ctl->m_r[r - 1];
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
     uint4 *out = (r & 1) ? a.wl1 : a.wl0;       // WL[r & 1]
-    const uint32_t ntiles = (uint32_t)((count + kTile - 1) / kTile);
+    const uint32_t rec_bytes = from_e0 ? (KIND == kKindMsf ? 12u : 8u) : 16u;
+    const uint32_t tile_bytes = kPipeTile * rec_bytes;
+    const char *src_base = from_e0 ? static_cast<const char *>(a.e0) : reinterpret_cast<const char *>(in);
+    const uint32_t ntiles = (uint32_t)((count + kPipeTile - 1) / kPipeTile);
+    const uint64_t full_tiles = count / kPipeTile;  // the partial last tile is read directly
     const uint32_t epoch = a.epoch_base + r;
-    for (;;) {
-        if (threadIdx.x == 0)
-            s_tile = atomicAdd(&ctl->ticket[r], 1u);
-        __syncthreads();
-        const uint32_t t = s_tile;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++)
+            mbar_init(&s_bar[s], 1);
+        fence_mbar_init();
+        for (int s = 0; s < kStages; s++) {
+            const uint32_t t = atomicAdd(&ctl->ticket[r], 1u);
+            s_tile[s] = t;
+            if (t < full_tiles) {
+                mbar_arrive_expect_tx(&s_bar[s], tile_bytes);
+                bulk_copy_g2s(stage_mem + s * kStageBytes, src_base + (uint64_t)t * tile_bytes, tile_bytes, &s_bar[s]);
+            }
+        }
+    }
+    __syncthreads();
+    uint32_t parity = 0;  // bit s: phase of stage s's barrier to wait for
+    for (uint32_t k = 0;; k++) {
+        const int s = (int)(k % kStages);
+        const uint32_t t = s_tile[s];
         if (t >= ntiles)
             break;
-        const uint64_t base = (uint64_t)t * kTile + (uint64_t)threadIdx.x * kItems;
-        uint32_t ra[4], rb[4], w[4], id[4];
-        bool keep[4];
-        if (from_e0) {
-            uint32_t u[4], v[4];
-            bool ok[4];
-            load4_e0<KIND>(a.e0, base, count, u, v, w, ok);
+        const bool bulk = t < full_tiles;
+        bool ok = true;
+        if (bulk) {
+            ok = mbar_wait(&s_bar[s], (parity >> s) & 1u, &ctl->err);
+            parity ^= 1u << s;
+        }
+        if (__syncthreads_or(!ok))
+            break;  // a bulk copy never completed; the status bit is set
+        const unsigned char *stage = stage_mem + s * kStageBytes;
+        const uint64_t tbase = (uint64_t)t * kPipeTile;
+        uint32_t ra[kPipeItems], rb[kPipeItems], w[kPipeItems], id[kPipeItems];
+        bool keep[kPipeItems];
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                bool live = ok[j] && e0_live<KIND>(u[j], v[j]);
-                if (live && (u[j] >= a.n || v[j] >= a.n)) {
+        for (int j = 0; j < kPipeItems; j++) {
+            const uint32_t idx = j * kBlock + threadIdx.x;
+            const uint64_t gi = tbase + idx;
+            const bool inb = gi < count;
+            if (from_e0) {
+                uint32_t u = 0, v = 0, ww = 0;
+                if (KIND == kKindMsf) {
+                    const uint32_t *p = bulk ? reinterpret_cast<const uint32_t *>(stage) + 3 * idx
+                                             : static_cast<const uint32_t *>(a.e0) + 3 * gi;
+                    if (inb) {
+                        u = p[0];
+                        v = p[1];
+                        ww = p[2];
+                    }
+                } else {
+                    const unsigned long long *p = bulk
+                                                      ? reinterpret_cast<const unsigned long long *>(stage) + idx
+                                                      : static_cast<const unsigned long long *>(a.e0) + gi;
+                    const unsigned long long e = inb ? *p : 0ull;
+                    u = (uint32_t)(e >> 32);
+                    v = (uint32_t)e;
+                }
+                bool live = inb && e0_live<KIND>(u, v);
+                if (live && (u >= a.n || v >= a.n)) {
                     if (src == kSrcLight)
                         set_err(&ctl->err, kErrRange);
                     live = false;
                 }
-                const bool light = e0_key<KIND>(w[j], base + j) < thr;
+                const bool light = e0_key<KIND>(ww, gi) < thr;
                 keep[j] = live && (src == kSrcLight ? light : !light);
-                ra[j] = u[j];
-                rb[j] = v[j];
-                id[j] = (uint32_t)(base + j);
-            }
-        } else {
-            const uint4 *q = in + base;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                keep[j] = base + j < count;
-                uint4 rec = keep[j] ? __ldcs(q + j) : make_uint4(0, 0, 0, 0);
+                ra[j] = u;
+                rb[j] = v;
+                w[j] = ww;
+                id[j] = (uint32_t)gi;
+            } else {
+                uint4 rec = make_uint4(0, 0, 0, 0);
+                if (inb)
+                    rec = bulk ? reinterpret_cast<const uint4 *>(stage)[idx] : __ldcs(in + gi);
+                keep[j] = inb;
                 ra[j] = rec.x;
                 rb[j] = rec.y;
                 w[j] = rec.z;
                 id[j] = rec.w;
             }
         }
-        uint32_t c = 0;
+        if (src != kSrcLight) {  // light round 0: every vertex is its own root
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if (keep[j] && src != kSrcLight) {  // light round 0: every vertex is its own root
-                ra[j] = __ldg(a.parent + ra[j]);
-                rb[j] = __ldg(a.parent + rb[j]);
-            }
-            keep[j] = keep[j] && ra[j] != rb[j];
-            c += keep[j];
+            for (int j = 0; j < kPipeItems; j++)
+                if (keep[j]) {
+                    ra[j] = __ldg(a.parent + ra[j]);
+                    rb[j] = __ldg(a.parent + rb[j]);
+                }
         }
-        uint32_t total;
-        const uint32_t off = block_exclusive_scan(c, &total, s_warp);
-        if (threadIdx.x < 32) {
+        unsigned mask[kPipeItems];
+#pragma unroll
+        for (int j = 0; j < kPipeItems; j++) {
+            keep[j] = keep[j] && ra[j] != rb[j];
+            mask[j] = __ballot_sync(0xffffffffu, keep[j]);
+        }
+        if (lane == 0)
+#pragma unroll
+            for (int j = 0; j < kPipeItems; j++)
+                s_cnt[j * kWarps + warp] = __popc(mask[j]);
+        __syncthreads();
+        if (warp == 0) {
+            // exclusive scan of the kPipeItems * kWarps (= 64) row/warp counts, row-major
+            const uint32_t c0 = s_cnt[2 * lane], c1 = s_cnt[2 * lane + 1];
+            const uint32_t sum = c0 + c1;
+            uint32_t incl = sum;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= (uint32_t)d)
+                    incl += y;
+            }
+            s_cnt[2 * lane] = incl - sum;
+            s_cnt[2 * lane + 1] = incl - sum + c0;
+            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
             const uint32_t ex = lookback_exclusive(a.status, t, total, epoch, &ctl->err);
-            if (threadIdx.x == 0) {
+            if (lane == 0) {
                 s_base = ex;
                 if (t == ntiles - 1)
                     ctl->m_r[r] = (unsigned long long)ex + total;
             }
         }
         __syncthreads();
-        uint32_t pos = s_base + off;
-        unsigned long long key[4];
+        const uint32_t base = s_base;
+        const unsigned below = (1u << lane) - 1u;
+        unsigned long long key[kPipeItems];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
+        for (int j = 0; j < kPipeItems; j++) {
+            const uint32_t pos = base + s_cnt[j * kWarps + warp] + __popc(mask[j] & below);
             key[j] = ((unsigned long long)w[j] << 32) | pos;
             if (keep[j])
                 out[pos] = make_uint4(ra[j], rb[j], w[j], id[j]);
-            pos += keep[j];
         }
-        offer4(a.best, ra, key, keep);
-        offer4(a.best, rb, key, keep);
+#pragma unroll
+        for (int h = 0; h < kPipeItems; h += 4) {
+            const uint32_t ta[4] = {ra[h], ra[h + 1], ra[h + 2], ra[h + 3]};
+            const uint32_t tb[4] = {rb[h], rb[h + 1], rb[h + 2], rb[h + 3]};
+            const unsigned long long kk[4] = {key[h], key[h + 1], key[h + 2], key[h + 3]};
+            const bool kp[4] = {keep[h], keep[h + 1], keep[h + 2], keep[h + 3]};
+            offer4(a.best, ta, kk, kp);
+            offer4(a.best, tb, kk, kp);
+        }
+        __syncthreads();  // the stage and s_cnt are free again
+        if (threadIdx.x == 0) {
+            const uint32_t t2 = atomicAdd(&ctl->ticket[r], 1u);
+            s_tile[s] = t2;
+            if (t2 < full_tiles) {
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&s_bar[s], tile_bytes);
+                bulk_copy_g2s(stage_mem + s * kStageBytes, src_base + (uint64_t)t2 * tile_bytes, tile_bytes,
+                              &s_bar[s]);
+            }
+        }
         __syncthreads();
     }
 }
@@ -588,7 +637,7 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
     const int vb = vertex_blocks(ctx, a.n);
     {
         KernelScope k(ctx, kKEdgePass);
-        edge_pass_kernel<KIND><<<ctx->edge_pass_blocks, kBlock, 0, ctx->stream>>>(a);
+        edge_pass_kernel<KIND><<<ctx->edge_pass_blocks, kBlock, kPipeSmem, ctx->stream>>>(a);
     }
     {
         KernelScope k(ctx, kKHook);
@@ -612,7 +661,12 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
     cudaStream_t s = ctx->stream;
     if (!ctx->edge_pass_blocks) {
         int per_sm = 0;
-        PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND>, kBlock, 0));
+        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kPipeSmem));
+        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem));
+        PHEM_CUDA_TRY(
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND>, kBlock, kPipeSmem));
         ctx->edge_pass_blocks = ctx->sm_count * std::max(1, per_sm);
         PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
         ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
