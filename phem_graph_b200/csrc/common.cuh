@@ -165,17 +165,21 @@ __device__ __forceinline__ uint64_t lb_word(uint64_t flag, uint32_t epoch, uint3
     return flag | ((uint64_t)(epoch & 0x3fffffffu) << 32) | value;
 }
 
-__device__ __forceinline__ uint32_t lookback_exclusive(uint64_t *status, uint32_t tile, uint32_t agg,
-                                                       uint32_t epoch, uint32_t *err)
+// First half: publish the tile's aggregate (tile 0 publishes its inclusive
+// prefix at once).  One lane calls it.
+__device__ __forceinline__ void lookback_publish(uint64_t *status, uint32_t tile, uint32_t agg, uint32_t epoch)
+{
+    st_relaxed_u64(status + tile, lb_word(tile == 0 ? kFlagIncl : kFlagAgg, epoch, agg));
+}
+
+// Second half: wait for the predecessors, publish the inclusive prefix and
+// return the exclusive one.  The whole warp calls it, after the publish.
+__device__ __forceinline__ uint32_t lookback_resolve(uint64_t *status, uint32_t tile, uint32_t agg, uint32_t epoch,
+                                                     uint32_t *err)
 {
     const uint32_t lane = lane_id();
-    if (tile == 0) {
-        if (lane == 0)
-            st_relaxed_u64(status, lb_word(kFlagIncl, epoch, agg));
+    if (tile == 0)
         return 0;
-    }
-    if (lane == 0)
-        st_relaxed_u64(status + tile, lb_word(kFlagAgg, epoch, agg));
     const uint32_t ep = epoch & 0x3fffffffu;
     uint32_t excl = 0;
     int64_t top = (int64_t)tile - 1;  // nearest predecessor not yet folded in
@@ -221,6 +225,16 @@ __device__ __forceinline__ uint32_t lookback_exclusive(uint64_t *status, uint32_
     if (lane == 0)
         st_relaxed_u64(status + tile, lb_word(kFlagIncl, epoch, excl + agg));
     return excl;
+}
+
+// Both halves back to back (warp-wide).
+__device__ __forceinline__ uint32_t lookback_exclusive(uint64_t *status, uint32_t tile, uint32_t agg,
+                                                       uint32_t epoch, uint32_t *err)
+{
+    if (lane_id() == 0)
+        lookback_publish(status, tile, agg, epoch);
+    __syncwarp();
+    return lookback_resolve(status, tile, agg, epoch, err);
 }
 
 // Grid size for the persistent streaming kernels: whole waves over 148 SMs.

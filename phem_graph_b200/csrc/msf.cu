@@ -223,21 +223,22 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
 }
 
 // One Boruvka round's edge pass: relabel + filter + stable compaction +
-// per-root minimum, as a software pipeline.  Each persistent CTA owns up to
-// kStages tiles of kPipeTile records at a time: whole tiles arrive in shared
-// memory by 1-D bulk copies (cp.async.bulk, completion on an mbarrier) while
-// the CTA works on an earlier tile, so HBM streaming overlaps the relabel
-// gathers, the scan and the look-back.  Threads read a tile striped (record
-// j * kBlock + tid), which is conflict-free for 8, 12 and 16-byte records, and
-// the stable rank of a survivor is its warp-ballot prefix plus a 64-entry scan
-// of the (row, warp) counts.  Tiles are numbered by tickets taken in order
-// when a stage is refilled, so the decoupled look-back only ever waits on
-// tiles that running CTAs already own.
+// per-root minimum, as a two-stage software pipeline.  Whole tiles of
+// kPipeTile records arrive in shared memory by 1-D bulk copies (cp.async.bulk,
+// completion on an mbarrier).  A CTA counts its current tile's survivors,
+// publishes that aggregate for the decoupled look-back, and only THEN takes
+// the next tile's ticket and starts its copy, which overlaps the look-back
+// wait, the survivor writes and the atomics of the current tile.  Taking a
+// ticket only after publishing keeps every claimed-but-unpublished tile at the
+// head of its CTA's queue, so no look-back chain forms across CTAs.  Threads
+// read a tile striped (record j * kBlock + tid), conflict-free for 8, 12 and
+// 16-byte records; the stable rank of a survivor is its warp-ballot prefix plus
+// a 64-entry scan of the (row, warp) counts.
 constexpr int kPipeTile = 2048;
 constexpr int kPipeItems = kPipeTile / kBlock;  // 8 records per thread
-constexpr int kStages = 3;
+constexpr int kStages = 2;
 constexpr size_t kStageBytes = (size_t)kPipeTile * 16;  // sized for the widest record
-constexpr size_t kPipeSmem = kStages * kStageBytes;     // 96 KB
+constexpr size_t kPipeSmem = kStages * kStageBytes;     // 64 KB
 
 template <int KIND>
 __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
@@ -269,19 +270,17 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         for (int s = 0; s < kStages; s++)
             mbar_init(&s_bar[s], 1);
         fence_mbar_init();
-        for (int s = 0; s < kStages; s++) {
-            const uint32_t t = atomicAdd(&ctl->ticket[r], 1u);
-            s_tile[s] = t;
-            if (t < full_tiles) {
-                mbar_arrive_expect_tx(&s_bar[s], tile_bytes);
-                bulk_copy_g2s(stage_mem + s * kStageBytes, src_base + (uint64_t)t * tile_bytes, tile_bytes, &s_bar[s]);
-            }
+        const uint32_t t = atomicAdd(&ctl->ticket[r], 1u);
+        s_tile[0] = t;
+        if (t < full_tiles) {
+            mbar_arrive_expect_tx(&s_bar[0], tile_bytes);
+            bulk_copy_g2s(stage_mem, src_base + (uint64_t)t * tile_bytes, tile_bytes, &s_bar[0]);
         }
     }
     __syncthreads();
     uint32_t parity = 0;  // bit s: phase of stage s's barrier to wait for
     for (uint32_t k = 0;; k++) {
-        const int s = (int)(k % kStages);
+        const int s = (int)(k & 1);
         const uint32_t t = s_tile[s];
         if (t >= ntiles)
             break;
@@ -376,7 +375,21 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             s_cnt[2 * lane] = incl - sum;
             s_cnt[2 * lane + 1] = incl - sum + c0;
             const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-            const uint32_t ex = lookback_exclusive(a.status, t, total, epoch, &ctl->err);
+            if (lane == 0) {
+                lookback_publish(a.status, t, total, epoch);
+                // next tile: ticket and bulk copy into the other stage (read last
+                // iteration, several barriers ago)
+                const uint32_t t2 = atomicAdd(&ctl->ticket[r], 1u);
+                s_tile[s ^ 1] = t2;
+                if (t2 < full_tiles) {
+                    fence_proxy_async_smem();
+                    mbar_arrive_expect_tx(&s_bar[s ^ 1], tile_bytes);
+                    bulk_copy_g2s(stage_mem + (s ^ 1) * kStageBytes, src_base + (uint64_t)t2 * tile_bytes,
+                                  tile_bytes, &s_bar[s ^ 1]);
+                }
+            }
+            __syncwarp();
+            const uint32_t ex = lookback_resolve(a.status, t, total, epoch, &ctl->err);
             if (lane == 0) {
                 s_base = ex;
                 if (t == ntiles - 1)
@@ -403,18 +416,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             offer4(a.best, ta, kk, kp);
             offer4(a.best, tb, kk, kp);
         }
-        __syncthreads();  // the stage and s_cnt are free again
-        if (threadIdx.x == 0) {
-            const uint32_t t2 = atomicAdd(&ctl->ticket[r], 1u);
-            s_tile[s] = t2;
-            if (t2 < full_tiles) {
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&s_bar[s], tile_bytes);
-                bulk_copy_g2s(stage_mem + s * kStageBytes, src_base + (uint64_t)t2 * tile_bytes, tile_bytes,
-                              &s_bar[s]);
-            }
-        }
-        __syncthreads();
+        __syncthreads();  // s_cnt and s_base are free again
     }
 }
 
