@@ -102,12 +102,20 @@ phem_status phem_context_set_profiling(phem_context *ctx, int on);
 phem_status phem_context_profile(phem_context *ctx, phem_kernel_profile *out, uint32_t max, uint32_t *count);
 phem_status phem_context_profile_reset(phem_context *ctx);
 
+/* Event-timed launches in launch order since the last reset (profiling on). */
+typedef struct phem_launch_record {
+    char name[32];
+    float ms;
+} phem_launch_record;
+phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, uint32_t max, uint32_t *count);
+
 /* Tuning knobs (defaults suit B200; the autotuner may change them):
  *   "msf.light_per_vertex"  light edges per vertex taken by the MSF filter
  *                           before the heavy pass; 0 disables the filter   [2.0]
  *   "msf.filter_min_ratio"  filter only when m >= ratio * light edges      [2.0]
  *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
  *   "msf.next_batch"        rounds queued per later check                 [4]
+ *   "msf.edge_items"        records per thread in the edge pass, 4 or 8   [8]
  * None of them changes a result. */
 phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double value);
 phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *value);

@@ -54,6 +54,10 @@ class KernelProfile(C.Structure):
                 ("total_ms", C.c_double)]
 
 
+class LaunchRecord(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("ms", C.c_float)]
+
+
 _VP = C.c_void_p
 _lib = None
 
@@ -73,6 +77,7 @@ SIGNATURES = {
     "phem_context_set_profiling": (C.c_int, [_VP, C.c_int]),
     "phem_context_profile": (C.c_int, [_VP, C.POINTER(KernelProfile), C.c_uint32, C.POINTER(C.c_uint32)]),
     "phem_context_profile_reset": (C.c_int, [_VP]),
+    "phem_context_launch_log": (C.c_int, [_VP, C.POINTER(LaunchRecord), C.c_uint32, C.POINTER(C.c_uint32)]),
     "phem_cc_solve": (C.c_int, [_VP, _VP, C.c_int64, C.c_int32, _VP, _VP, C.c_uint32, C.POINTER(CCStats)]),
     "phem_cc_init": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
     "phem_cc_unite": (C.c_int, [_VP, _VP, C.c_int64, C.c_int32, _VP, _VP]),

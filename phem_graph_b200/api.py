@@ -117,6 +117,15 @@ class Context:
     def launches(self) -> int:
         return sum(v["launches"] for v in self.profile().values())
 
+    def launch_log(self) -> list:
+        """[(kernel name, ms)] of the event-timed launches since the last reset."""
+        from ._lib import LaunchRecord
+        cnt = C.c_uint32()
+        check(lib().phem_context_launch_log(self._h, None, 0, C.byref(cnt)), "phem_context_launch_log")
+        buf = (LaunchRecord * max(cnt.value, 1))()
+        check(lib().phem_context_launch_log(self._h, buf, cnt.value, C.byref(cnt)), "phem_context_launch_log")
+        return [(buf[i].name.decode(), float(buf[i].ms)) for i in range(cnt.value)]
+
     # ------------------------------------------------------------ CC
     def cc_solve(self, edges, n: int, canonical: bool = False, labels=None, forest=None,
                  want_forest: bool = True) -> CCResult:

@@ -73,6 +73,8 @@ const char *const kKernelNames[kKernelCount] = {
     "msf_init", "msf_select", "msf_edge_pass", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
     "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "csr_pack"};
 
+constexpr size_t kLaunchLogCap = 1u << 16;
+
 static cudaEvent_t pool_get(phem_context *ctx)
 {
     if (!ctx->event_pool.empty()) {
@@ -118,6 +120,8 @@ void resolve_timings(phem_context *ctx)
         if (cudaEventSynchronize(p.stop) == cudaSuccess && cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
             ctx->kernel_ms[p.kernel] += ms;
             ctx->timed_launches[p.kernel]++;
+            if (ctx->launch_log.size() < kLaunchLogCap)
+                ctx->launch_log.emplace_back(p.kernel, ms);
         }
         ctx->event_pool.push_back(p.start);
         ctx->event_pool.push_back(p.stop);
@@ -446,6 +450,24 @@ phem_status phem_context_profile_reset(phem_context *ctx)
         ctx->timed_launches[i] = 0;
         ctx->kernel_ms[i] = 0;
     }
+    ctx->launch_log.clear();
+    return PHEM_OK;
+}
+
+phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, uint32_t max, uint32_t *count)
+{
+    PHEM_TRY(check_ctx(ctx));
+    DeviceGuard g(ctx->device);
+    PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    resolve_timings(ctx);
+    const uint32_t n = (uint32_t)ctx->launch_log.size();
+    for (uint32_t i = 0; out && i < n && i < max; i++) {
+        std::memset(&out[i], 0, sizeof(out[i]));
+        std::snprintf(out[i].name, sizeof(out[i].name), "%s", kKernelNames[ctx->launch_log[i].first]);
+        out[i].ms = ctx->launch_log[i].second;
+    }
+    if (count)
+        *count = n;
     return PHEM_OK;
 }
 
@@ -465,6 +487,8 @@ phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double v
         ctx->tune_first_batch = (int)value;
     } else if (k == "msf.next_batch" && value >= 1 && value <= PHEM_MAX_ROUNDS) {
         ctx->tune_next_batch = (int)value;
+    } else if (k == "msf.edge_items" && (value == 4 || value == 8)) {
+        ctx->tune_edge_items = (int)value;
     } else {
         set_error("set_tuning: unknown key or value out of range: %s = %g", key, value);
         return PHEM_ERR_INVALID;
@@ -488,6 +512,8 @@ phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *
         *value = ctx->tune_first_batch;
     else if (k == "msf.next_batch")
         *value = ctx->tune_next_batch;
+    else if (k == "msf.edge_items")
+        *value = ctx->tune_edge_items;
     else {
         set_error("get_tuning: unknown key %s", key);
         return PHEM_ERR_INVALID;

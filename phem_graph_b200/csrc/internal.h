@@ -42,7 +42,9 @@ struct phem_context {
     uint32_t timeout_ms = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     int edge_pass_blocks = 0;          // persistent grid sizes, from the occupancy API
+    int edge_pass_blocks4 = 0;
     int gather_blocks = 0;
+    int tune_edge_items = 8;             // records per thread in the MSF edge pass (4 or 8)
     // tuning knobs (phem_context_set_tuning)
     double tune_light_per_vertex = 2.0;  // light edges per vertex in the MSF filter (0: no filter)
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
@@ -55,6 +57,7 @@ struct phem_context {
     bool profiling = false;
     std::vector<phem::PendingTiming> pending;
     std::vector<cudaEvent_t> event_pool;
+    std::vector<std::pair<int, float>> launch_log;  // (kernel, ms) of timed launches, oldest first
 };
 
 namespace phem {

@@ -77,38 +77,6 @@ __device__ __forceinline__ unsigned long long e0_key(uint32_t w, uint64_t id)
     return KIND == kKindMsf ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
 }
 
-// Offers key k[j] to best[t[j]] for live slots j: equal targets among the four
-// are folded first, then every guard load is issued before any atomic, so the
-// four L2 round trips overlap.  The guard read may be stale but never below
-// the true minimum, so it only skips atomics that could not lower it.
-__device__ __forceinline__ void offer4(unsigned long long *best, const uint32_t (&t)[4],
-                                       const unsigned long long (&k)[4], const bool (&ok)[4])
-{
-    bool o[4];
-    unsigned long long kk[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        o[j] = ok[j];
-        kk[j] = k[j];
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-        for (int i = j + 1; i < 4; i++)
-            if (o[j] && o[i] && t[i] == t[j]) {
-                kk[j] = kk[i] < kk[j] ? kk[i] : kk[j];
-                o[i] = false;
-            }
-    unsigned long long g[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-        g[j] = o[j] ? __ldcg(best + t[j]) : 0ull;
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-        if (o[j] && kk[j] < g[j])
-            atomicMin(best + t[j], kk[j]);
-}
-
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
 {
 #pragma unroll
@@ -234,19 +202,44 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
 // read a tile striped (record j * kBlock + tid), conflict-free for 8, 12 and
 // 16-byte records; the stable rank of a survivor is its warp-ballot prefix plus
 // a 64-entry scan of the (row, warp) counts.
-constexpr int kPipeTile = 2048;
-constexpr int kPipeItems = kPipeTile / kBlock;  // 8 records per thread
 constexpr int kStages = 2;
-constexpr size_t kStageBytes = (size_t)kPipeTile * 16;  // sized for the widest record
-constexpr size_t kPipeSmem = kStages * kStageBytes;     // 64 KB
+constexpr int kMaxItems = 8;
+constexpr size_t kStageBytes = (size_t)kBlock * kMaxItems * 16;  // sized for the widest record
+constexpr size_t kPipeSmem = kStages * kStageBytes;                // 64 KB
 
-template <int KIND>
-__global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
+// Offers key k to best[t] for the lanes with `live`.  When every live lane of
+// the warp has the same target (a hub's run in row-major input) the warp
+// reduces first and one lane does the atomic; otherwise each live lane whose
+// key beats its (possibly stale, never too low) guard value does its own.
+__device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, unsigned long long k, bool live,
+                                          unsigned long long guard)
 {
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (!act)
+        return;
+    const int leader = __ffs(act) - 1;
+    const uint32_t t0 = __shfl_sync(0xffffffffu, t, leader);
+    if (__all_sync(0xffffffffu, !live || t == t0)) {
+        const uint32_t hi = live ? (uint32_t)(k >> 32) : 0xffffffffu, lo = (uint32_t)k;
+        const uint32_t mhi = __reduce_min_sync(0xffffffffu, hi);
+        const uint32_t mlo = __reduce_min_sync(0xffffffffu, live && hi == mhi ? lo : 0xffffffffu);
+        const unsigned long long km = ((unsigned long long)mhi << 32) | mlo;
+        if ((int)lane_id() == leader && km < guard)
+            atomicMin(best + t0, km);
+    } else if (live && k < guard) {
+        atomicMin(best + t, k);
+    }
+}
+
+template <int KIND, int ITEMS>
+__global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(RoundArgs a)
+{
+    constexpr int kTileRecs = kBlock * ITEMS;
+    constexpr int kCnt = ITEMS * kWarps;  // row/warp counts per tile
     extern __shared__ __align__(128) unsigned char stage_mem[];
     __shared__ uint64_t s_bar[kStages];
     __shared__ uint32_t s_tile[kStages];
-    __shared__ uint32_t s_cnt[kPipeItems * kWarps];
+    __shared__ uint32_t s_cnt[kCnt];
     __shared__ uint32_t s_base;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
@@ -259,10 +252,10 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
     uint4 *out = (r & 1) ? a.wl1 : a.wl0;       // WL[r & 1]
     const uint32_t rec_bytes = from_e0 ? (KIND == kKindMsf ? 12u : 8u) : 16u;
-    const uint32_t tile_bytes = kPipeTile * rec_bytes;
+    const uint32_t tile_bytes = kTileRecs * rec_bytes;
     const char *src_base = from_e0 ? static_cast<const char *>(a.e0) : reinterpret_cast<const char *>(in);
-    const uint32_t ntiles = (uint32_t)((count + kPipeTile - 1) / kPipeTile);
-    const uint64_t full_tiles = count / kPipeTile;  // the partial last tile is read directly
+    const uint32_t ntiles = (uint32_t)((count + kTileRecs - 1) / kTileRecs);
+    const uint64_t full_tiles = count / kTileRecs;  // the partial last tile is read directly
     const uint32_t epoch = a.epoch_base + r;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
 
@@ -293,11 +286,11 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         if (__syncthreads_or(!ok))
             break;  // a bulk copy never completed; the status bit is set
         const unsigned char *stage = stage_mem + s * kStageBytes;
-        const uint64_t tbase = (uint64_t)t * kPipeTile;
-        uint32_t ra[kPipeItems], rb[kPipeItems], w[kPipeItems], id[kPipeItems];
-        bool keep[kPipeItems];
+        const uint64_t tbase = (uint64_t)t * kTileRecs;
+        uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
+        bool keep[ITEMS];
 #pragma unroll
-        for (int j = 0; j < kPipeItems; j++) {
+        for (int j = 0; j < ITEMS; j++) {
             const uint32_t idx = j * kBlock + threadIdx.x;
             const uint64_t gi = tbase + idx;
             const bool inb = gi < count;
@@ -344,27 +337,36 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         }
         if (src != kSrcLight) {  // light round 0: every vertex is its own root
 #pragma unroll
-            for (int j = 0; j < kPipeItems; j++)
+            for (int j = 0; j < ITEMS; j++)
                 if (keep[j]) {
                     ra[j] = __ldg(a.parent + ra[j]);
                     rb[j] = __ldg(a.parent + rb[j]);
                 }
         }
-        unsigned mask[kPipeItems];
+        unsigned mask[ITEMS];
+        unsigned long long ga[ITEMS], gb[ITEMS];
 #pragma unroll
-        for (int j = 0; j < kPipeItems; j++) {
+        for (int j = 0; j < ITEMS; j++) {
             keep[j] = keep[j] && ra[j] != rb[j];
             mask[j] = __ballot_sync(0xffffffffu, keep[j]);
+            // guard values travel while warp 0 scans and waits on the look-back
+            ga[j] = keep[j] ? __ldcg(a.best + ra[j]) : 0ull;
+            gb[j] = keep[j] ? __ldcg(a.best + rb[j]) : 0ull;
         }
         if (lane == 0)
 #pragma unroll
-            for (int j = 0; j < kPipeItems; j++)
+            for (int j = 0; j < ITEMS; j++)
                 s_cnt[j * kWarps + warp] = __popc(mask[j]);
         __syncthreads();
         if (warp == 0) {
-            // exclusive scan of the kPipeItems * kWarps (= 64) row/warp counts, row-major
-            const uint32_t c0 = s_cnt[2 * lane], c1 = s_cnt[2 * lane + 1];
-            const uint32_t sum = c0 + c1;
+            // exclusive scan of the row/warp counts, row-major, kCnt / 32 per lane
+            constexpr int kPer = kCnt / 32;
+            uint32_t c[kPer], sum = 0;
+#pragma unroll
+            for (int q = 0; q < kPer; q++) {
+                c[q] = s_cnt[kPer * lane + q];
+                sum += c[q];
+            }
             uint32_t incl = sum;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
@@ -372,8 +374,12 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                 if (lane >= (uint32_t)d)
                     incl += y;
             }
-            s_cnt[2 * lane] = incl - sum;
-            s_cnt[2 * lane + 1] = incl - sum + c0;
+            uint32_t run = incl - sum;
+#pragma unroll
+            for (int q = 0; q < kPer; q++) {
+                s_cnt[kPer * lane + q] = run;
+                run += c[q];
+            }
             const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
             if (lane == 0) {
                 lookback_publish(a.status, t, total, epoch);
@@ -399,22 +405,14 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         __syncthreads();
         const uint32_t base = s_base;
         const unsigned below = (1u << lane) - 1u;
-        unsigned long long key[kPipeItems];
 #pragma unroll
-        for (int j = 0; j < kPipeItems; j++) {
+        for (int j = 0; j < ITEMS; j++) {
             const uint32_t pos = base + s_cnt[j * kWarps + warp] + __popc(mask[j] & below);
-            key[j] = ((unsigned long long)w[j] << 32) | pos;
+            const unsigned long long key = ((unsigned long long)w[j] << 32) | pos;
             if (keep[j])
                 out[pos] = make_uint4(ra[j], rb[j], w[j], id[j]);
-        }
-#pragma unroll
-        for (int h = 0; h < kPipeItems; h += 4) {
-            const uint32_t ta[4] = {ra[h], ra[h + 1], ra[h + 2], ra[h + 3]};
-            const uint32_t tb[4] = {rb[h], rb[h + 1], rb[h + 2], rb[h + 3]};
-            const unsigned long long kk[4] = {key[h], key[h + 1], key[h + 2], key[h + 3]};
-            const bool kp[4] = {keep[h], keep[h + 1], keep[h + 2], keep[h + 3]};
-            offer4(a.best, ta, kk, kp);
-            offer4(a.best, tb, kk, kp);
+            offer_row(a.best, ra[j], key, keep[j], ga[j]);
+            offer_row(a.best, rb[j], key, keep[j], gb[j]);
         }
         __syncthreads();  // s_cnt and s_base are free again
     }
@@ -639,7 +637,10 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
     const int vb = vertex_blocks(ctx, a.n);
     {
         KernelScope k(ctx, kKEdgePass);
-        edge_pass_kernel<KIND><<<ctx->edge_pass_blocks, kBlock, kPipeSmem, ctx->stream>>>(a);
+        if (ctx->tune_edge_items == 4)
+            edge_pass_kernel<KIND, 4><<<ctx->edge_pass_blocks4, kBlock, kPipeSmem / 2, ctx->stream>>>(a);
+        else
+            edge_pass_kernel<KIND, 8><<<ctx->edge_pass_blocks, kBlock, kPipeSmem, ctx->stream>>>(a);
     }
     {
         KernelScope k(ctx, kKHook);
@@ -663,13 +664,20 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
     cudaStream_t s = ctx->stream;
     if (!ctx->edge_pass_blocks) {
         int per_sm = 0;
-        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kPipeSmem));
-        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked>,
+        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf, 8>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem));
+        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked, 8>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem));
+        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf, 4>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem / 2));
+        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked, 4>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem / 2));
         PHEM_CUDA_TRY(
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND>, kBlock, kPipeSmem));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 8>, kBlock, kPipeSmem));
         ctx->edge_pass_blocks = ctx->sm_count * std::max(1, per_sm);
+        PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 4>, kBlock,
+                                                                    kPipeSmem / 2));
+        ctx->edge_pass_blocks4 = ctx->sm_count * std::max(1, per_sm);
         PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
         ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
     }
