@@ -203,9 +203,19 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
 // 16-byte records; the stable rank of a survivor is its warp-ballot prefix plus
 // a 64-entry scan of the (row, warp) counts.
 constexpr int kStages = 2;
-constexpr int kMaxItems = 8;
-constexpr size_t kStageBytes = (size_t)kBlock * kMaxItems * 16;  // sized for the widest record
-constexpr size_t kPipeSmem = kStages * kStageBytes;                // 64 KB
+// Shared memory of one stage and of the whole pipeline for ITEMS records per
+// thread, sized for the widest (16-byte) record.  The launch passes
+// pipe_smem<ITEMS>() and the kernel indexes stages with stage_bytes<ITEMS>().
+template <int ITEMS>
+constexpr size_t stage_bytes()
+{
+    return (size_t)kBlock * ITEMS * 16;
+}
+template <int ITEMS>
+constexpr size_t pipe_smem()
+{
+    return kStages * stage_bytes<ITEMS>();
+}
 
 // Offers key k to best[t] for the lanes with `live`.  When every live lane of
 // the warp has the same target (a hub's run in row-major input) the warp
@@ -285,7 +295,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
         }
         if (__syncthreads_or(!ok))
             break;  // a bulk copy never completed; the status bit is set
-        const unsigned char *stage = stage_mem + s * kStageBytes;
+        const unsigned char *stage = stage_mem + s * stage_bytes<ITEMS>();
         const uint64_t tbase = (uint64_t)t * kTileRecs;
         uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
         bool keep[ITEMS];
@@ -390,7 +400,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
                 if (t2 < full_tiles) {
                     fence_proxy_async_smem();
                     mbar_arrive_expect_tx(&s_bar[s ^ 1], tile_bytes);
-                    bulk_copy_g2s(stage_mem + (s ^ 1) * kStageBytes, src_base + (uint64_t)t2 * tile_bytes,
+                    bulk_copy_g2s(stage_mem + (s ^ 1) * stage_bytes<ITEMS>(), src_base + (uint64_t)t2 * tile_bytes,
                                   tile_bytes, &s_bar[s ^ 1]);
                 }
             }
@@ -638,9 +648,9 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
     {
         KernelScope k(ctx, kKEdgePass);
         if (ctx->tune_edge_items == 4)
-            edge_pass_kernel<KIND, 4><<<ctx->edge_pass_blocks4, kBlock, kPipeSmem / 2, ctx->stream>>>(a);
+            edge_pass_kernel<KIND, 4><<<ctx->edge_pass_blocks4, kBlock, pipe_smem<4>(), ctx->stream>>>(a);
         else
-            edge_pass_kernel<KIND, 8><<<ctx->edge_pass_blocks, kBlock, kPipeSmem, ctx->stream>>>(a);
+            edge_pass_kernel<KIND, 8><<<ctx->edge_pass_blocks, kBlock, pipe_smem<8>(), ctx->stream>>>(a);
     }
     {
         KernelScope k(ctx, kKHook);
@@ -665,18 +675,18 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
     if (!ctx->edge_pass_blocks) {
         int per_sm = 0;
         PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf, 8>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem));
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<8>()));
         PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked, 8>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem));
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<8>()));
         PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf, 4>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem / 2));
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<4>()));
         PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked, 4>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem / 2));
-        PHEM_CUDA_TRY(
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 8>, kBlock, kPipeSmem));
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<4>()));
+        PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 8>, kBlock,
+                                                                    pipe_smem<8>()));
         ctx->edge_pass_blocks = ctx->sm_count * std::max(1, per_sm);
         PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 4>, kBlock,
-                                                                    kPipeSmem / 2));
+                                                                    pipe_smem<4>()));
         ctx->edge_pass_blocks4 = ctx->sm_count * std::max(1, per_sm);
         PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
         ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);

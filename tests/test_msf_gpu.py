@@ -161,3 +161,24 @@ def test_repeated_solves_share_context(ctx):
         E = g.msf_edges()
         ids, cnt, tot = expect(E, g.n)
         assert_msf(ctx.msf_solve(E, g.n), E, ids, cnt, tot)
+
+
+@pytest.mark.parametrize("items", [4, 8])
+def test_edge_items_variants(ctx, items):
+    """Both edge-pass instantiations (4 and 8 records per thread) give the same
+    forest, for weighted and for packed (canonical CC) edges."""
+    g = gen.rmat_graph(15, 16, seed=5)
+    E = g.msf_edges()
+    ids, cnt, tot = expect(E, g.n)
+    c = gen.er_graph(1 << 15, 1 << 17, seed=6)
+    labels, forest = oracle.cc_solve(c.pairs, c.n)
+    old = ctx.get_tuning("msf.edge_items")
+    ctx.set_tuning("msf.edge_items", items)
+    try:
+        r = ctx.msf_solve(E, g.n)
+        rc = ctx.cc_solve(c.pairs, c.n, canonical=True)
+    finally:
+        ctx.set_tuning("msf.edge_items", old)
+    assert_msf(r, E, ids, cnt, tot)
+    np.testing.assert_array_equal(rc.labels, labels)
+    np.testing.assert_array_equal(P.api.forest_set(rc.forest), oracle.forest_set(forest))
