@@ -43,6 +43,7 @@ struct phem_context {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     int edge_pass_blocks = 0;          // persistent grid sizes, from the occupancy API
     int edge_pass_blocks4 = 0;
+    uint32_t kernels_ready = 0;        // bit k: launch attributes of edge kind k are set
     int gather_blocks = 0;
     int tune_edge_items = 8;             // records per thread in the MSF edge pass (4 or 8)
     // tuning knobs (phem_context_set_tuning)

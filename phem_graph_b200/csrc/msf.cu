@@ -12,29 +12,32 @@
 //
 // Order of work (B200 design, not a translation):
 //   1. A one-CTA kernel picks a weight threshold from a stratified sample of
-//      the input so that about `light_per_vertex * n` edges are light.  This is
-//      the filtering step of PBBS mst() (approximate k-th smallest, :805-813),
-//      done on the device.
-//   2. Light phase.  Round 0 streams the input once with 128-bit loads and
-//      keeps only light edges; later rounds stream the (small) survivor list.
-//      Each round is ONE pass: relabel both endpoints to their roots, drop
-//      internal edges, write survivors as 16-byte {root_u, root_v, w, id}
-//      records with a stable single-pass compaction (decoupled look-back), and
-//      offer each survivor's key to both roots in the same pass.  Because the
-//      compaction is stable a survivor's position orders like its id, so keys
-//      carry (w, position) and the hook step reads the record directly.
+//      the input so that about `light_per_vertex * n` edges are light: the
+//      filtering step of PBBS mst() (approximate k-th smallest, :805-813), done
+//      on the device.
+//   2. Light phase.  Round 0 streams the input once and keeps only light
+//      edges; later rounds stream the (small) survivor list.  Each round is ONE
+//      pass: relabel both endpoints to their roots, drop internal edges, append
+//      survivors as 16-byte {root_u, root_v, w, id} records, and offer each
+//      survivor to both roots.
 //   3. When no light edge is left the parents of all vertices are compressed
 //      and the input is streamed a second time keeping heavy edges whose
 //      endpoints lie in different components (PBBS's second filter, :819-823);
-//      Boruvka continues on those survivors.
-//   An edge that is heavy and internal after the light phase closes a cycle of
-//   lighter edges, so it is in no MSF: the filter changes the work, not the
-//   result.
-// MSF membership is a bitmap over edge ids; one ordered gather writes the MSF
-// records ascending by id with the uint64 total.  Every kernel reads the
-// round, phase and continue flag from the device control block, so rounds are
-// queued ahead without host round trips; a round queued after convergence
-// exits at once.
+//      Boruvka continues on those survivors.  An edge that is heavy and
+//      internal after the light phase closes a cycle of lighter edges, so it
+//      is in no MSF: the filter changes the work, not the result.
+//
+// Each component's choice lives in a 16-byte slot {key = w << 32 | id, the far
+// root} updated with a 128-bit compare-and-swap, so the hook step needs no
+// survivor record and the survivor list may be in any order.  That removes
+// every dependency between CTAs from the edge pass: tiles are statically
+// strided over a persistent grid, arrive in shared memory by 1-D bulk copies
+// (cp.async.bulk) two tiles ahead of use, and each tile reserves its output
+// range with one atomicAdd.  MSF membership is a bitmap over edge ids; one
+// ordered gather (decoupled look-back) writes the MSF records ascending by id
+// with the uint64 total.  Every round kernel reads the round, phase and
+// continue flag from the device control block, so rounds are queued ahead
+// without host round trips; a round queued after convergence exits at once.
 #include <algorithm>
 #include <cstring>
 
@@ -49,7 +52,7 @@ struct RoundArgs {
     uint32_t n;
     uint32_t epoch_base;
     uint32_t *parent;
-    unsigned long long *best;
+    ulonglong2 *best;  // per component: {key, far root}
     uint32_t *cand0, *cand1;
     uint32_t *bitmap;
     uint4 *wl0, *wl1;
@@ -57,8 +60,6 @@ struct RoundArgs {
     unsigned long long *forest;
     Ctl *ctl;
 };
-
-// ---- input record access --------------------------------------------------
 
 // An input record takes part in the forest: self-loops never do; packed CC
 // edges follow union_find_gpu_COO and only count when u < v
@@ -69,12 +70,77 @@ __device__ __forceinline__ bool e0_live(uint32_t u, uint32_t v)
     return KIND == kKindMsf ? (u != v) : (u < v);
 }
 
-// Key that decides light/heavy: (w, id) for weighted edges, id for packed CC
-// edges (the canonical forest orders edges by index alone).
+// Key of an edge: (w, id) for weighted edges, id alone for packed CC edges
+// (the canonical forest orders edges by index).
 template <int KIND>
 __device__ __forceinline__ unsigned long long e0_key(uint32_t w, uint64_t id)
 {
     return KIND == kKindMsf ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
+}
+
+__device__ __forceinline__ ulonglong2 ld_cg_slot(const ulonglong2 *p)
+{
+    return __ldcg(p);
+}
+
+__device__ __forceinline__ ulonglong2 cas128(ulonglong2 *addr, ulonglong2 cmp, ulonglong2 val)
+{
+    ulonglong2 old;
+    asm volatile(
+        "{\n\t.reg .b128 c, v, o;\n\t"
+        "mov.b128 c, {%2, %3};\n\t"
+        "mov.b128 v, {%4, %5};\n\t"
+        "atom.global.cas.b128 o, [%6], c, v;\n\t"
+        "mov.b128 {%0, %1}, o;\n\t}"
+        : "=l"(old.x), "=l"(old.y)
+        : "l"(cmp.x), "l"(cmp.y), "l"(val.x), "l"(val.y), "l"(addr)
+        : "memory");
+    return old;
+}
+
+constexpr uint32_t kCasCap = 1u << 16;
+
+// Lowers slot t to {key, far} if key is smaller.  `guard` is an earlier read
+// of the slot's key: it may be stale but never below the true one, so it only
+// skips updates that could not win.
+__device__ __forceinline__ void slot_min(ulonglong2 *best, uint32_t t, unsigned long long key, uint32_t far,
+                                         unsigned long long guard, uint32_t *err)
+{
+    if (key >= guard)
+        return;
+    ulonglong2 cur = ld_cg_slot(best + t);
+    const ulonglong2 mine = make_ulonglong2(key, far);
+    for (uint32_t i = 0; i < kCasCap; i++) {
+        if (key >= cur.x)
+            return;
+        const ulonglong2 old = cas128(best + t, cur, mine);
+        if (old.x == cur.x && old.y == cur.y)
+            return;
+        cur = old;
+    }
+    set_err(err, kErrRetry);
+}
+
+// Offers edge (key, far) to slot t for the live lanes of a warp.  When every
+// live lane has the same target (a hub's run in row-major input) the warp
+// reduces the key first and only the winning lane updates the slot.
+__device__ __forceinline__ void offer_row(ulonglong2 *best, uint32_t t, unsigned long long key, uint32_t far,
+                                          bool live, unsigned long long guard, uint32_t *err)
+{
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (!act)
+        return;
+    const uint32_t t0 = __shfl_sync(0xffffffffu, t, __ffs(act) - 1);
+    if (__all_sync(0xffffffffu, !live || t == t0)) {
+        const uint32_t hi = live ? (uint32_t)(key >> 32) : 0xffffffffu;
+        const uint32_t lo = live ? (uint32_t)key : 0xffffffffu;
+        const uint32_t mhi = __reduce_min_sync(0xffffffffu, hi);
+        const uint32_t mlo = __reduce_min_sync(0xffffffffu, hi == mhi ? lo : 0xffffffffu);
+        if (live && hi == mhi && lo == mlo)  // keys are unique: exactly one lane
+            slot_min(best, t, key, far, guard, err);
+    } else if (live) {
+        slot_min(best, t, key, far, guard, err);
+    }
 }
 
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
@@ -107,7 +173,7 @@ __global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a, unsigned long
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.n; x += stride) {
         a.parent[x] = x;
-        a.best[x] = kKeyNone;
+        a.best[x] = make_ulonglong2(kKeyNone, 0);
         if (a.forest)
             a.forest[x] = kForestEmpty;
     }
@@ -144,9 +210,9 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
         s_prefix = 0;
         s_rank = (uint32_t)(k * kSample / m);
     }
-    const int shifts[3] = {21, 10, 0}, bits[3] = {11, 11, 10};
+#pragma unroll
     for (int d = 0; d < 3; d++) {
-        const int sh = shifts[d], nb = bits[d], hsh = sh + nb;
+        const int sh = d == 0 ? 21 : (d == 1 ? 10 : 0), nb = d == 2 ? 10 : 11, hsh = sh + nb;
         for (int i = tid; i < 2048; i += kSelectThreads)
             hist[i] = 0;
         __syncthreads();
@@ -165,13 +231,12 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
             uint32_t incl = sum;
 #pragma unroll
             for (int s = 1; s < 32; s <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, incl, s);
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, s);
                 if (tid >= s)
                     incl += y;
             }
             const uint32_t excl = incl - sum, rank = s_rank;
-            const bool mine = rank >= excl && rank < incl;
-            if (mine) {
+            if (rank >= excl && rank < incl) {
                 uint32_t c = excl;
                 for (int b = 0; b < 64; b++) {
                     const uint32_t h = hist[tid * 64 + b];
@@ -190,65 +255,34 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
         ctl->threshold = (unsigned long long)s_prefix << 32;
 }
 
-// One Boruvka round's edge pass: relabel + filter + stable compaction +
-// per-root minimum, as a two-stage software pipeline.  Whole tiles of
-// kPipeTile records arrive in shared memory by 1-D bulk copies (cp.async.bulk,
-// completion on an mbarrier).  A CTA counts its current tile's survivors,
-// publishes that aggregate for the decoupled look-back, and only THEN takes
-// the next tile's ticket and starts its copy, which overlaps the look-back
-// wait, the survivor writes and the atomics of the current tile.  Taking a
-// ticket only after publishing keeps every claimed-but-unpublished tile at the
-// head of its CTA's queue, so no look-back chain forms across CTAs.  Threads
-// read a tile striped (record j * kBlock + tid), conflict-free for 8, 12 and
-// 16-byte records; the stable rank of a survivor is its warp-ballot prefix plus
-// a 64-entry scan of the (row, warp) counts.
-constexpr int kStages = 2;
-// Shared memory of one stage and of the whole pipeline for ITEMS records per
-// thread, sized for the widest (16-byte) record.  The launch passes
-// pipe_smem<ITEMS>() and the kernel indexes stages with stage_bytes<ITEMS>().
+// One Boruvka round's edge pass: relabel + filter + compaction + per-root
+// minimum.  Tile k of a CTA is tile blockIdx.x + k * gridDim.x; stage k % 3 of
+// shared memory receives it by bulk copy two iterations ahead.  Threads read
+// a tile striped (record j * kBlock + tid), conflict-free for 8, 12 and
+// 16-byte records.  Survivor ranks inside the tile come from warp ballots and
+// a scan of the (row, warp) counts; warp 0 reserves the tile's output range
+// with one atomicAdd on the round's counter while every warp is already
+// updating component slots.
+constexpr int kStages = 3;
+
 template <int ITEMS>
-constexpr size_t stage_bytes()
+__host__ __device__ constexpr size_t stage_bytes()
 {
-    return (size_t)kBlock * ITEMS * 16;
+    return (size_t)kBlock * ITEMS * 16;  // sized for the widest (16-byte) record
 }
 template <int ITEMS>
-constexpr size_t pipe_smem()
+__host__ __device__ constexpr size_t pipe_smem()
 {
     return kStages * stage_bytes<ITEMS>();
 }
 
-// Offers key k to best[t] for the lanes with `live`.  When every live lane of
-// the warp has the same target (a hub's run in row-major input) the warp
-// reduces first and one lane does the atomic; otherwise each live lane whose
-// key beats its (possibly stale, never too low) guard value does its own.
-__device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, unsigned long long k, bool live,
-                                          unsigned long long guard)
-{
-    const unsigned act = __ballot_sync(0xffffffffu, live);
-    if (!act)
-        return;
-    const int leader = __ffs(act) - 1;
-    const uint32_t t0 = __shfl_sync(0xffffffffu, t, leader);
-    if (__all_sync(0xffffffffu, !live || t == t0)) {
-        const uint32_t hi = live ? (uint32_t)(k >> 32) : 0xffffffffu, lo = (uint32_t)k;
-        const uint32_t mhi = __reduce_min_sync(0xffffffffu, hi);
-        const uint32_t mlo = __reduce_min_sync(0xffffffffu, live && hi == mhi ? lo : 0xffffffffu);
-        const unsigned long long km = ((unsigned long long)mhi << 32) | mlo;
-        if ((int)lane_id() == leader && km < guard)
-            atomicMin(best + t0, km);
-    } else if (live && k < guard) {
-        atomicMin(best + t, k);
-    }
-}
-
 template <int KIND, int ITEMS>
-__global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(RoundArgs a)
+__global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
 {
     constexpr int kTileRecs = kBlock * ITEMS;
     constexpr int kCnt = ITEMS * kWarps;  // row/warp counts per tile
     extern __shared__ __align__(128) unsigned char stage_mem[];
     __shared__ uint64_t s_bar[kStages];
-    __shared__ uint32_t s_tile[kStages];
     __shared__ uint32_t s_cnt[kCnt];
     __shared__ uint32_t s_base;
     Ctl *ctl = a.ctl;
@@ -264,29 +298,28 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
     const uint32_t rec_bytes = from_e0 ? (KIND == kKindMsf ? 12u : 8u) : 16u;
     const uint32_t tile_bytes = kTileRecs * rec_bytes;
     const char *src_base = from_e0 ? static_cast<const char *>(a.e0) : reinterpret_cast<const char *>(in);
-    const uint32_t ntiles = (uint32_t)((count + kTileRecs - 1) / kTileRecs);
+    const uint64_t ntiles = (count + kTileRecs - 1) / kTileRecs;
     const uint64_t full_tiles = count / kTileRecs;  // the partial last tile is read directly
-    const uint32_t epoch = a.epoch_base + r;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    unsigned long long *counter = &ctl->m_r[r];
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++)
             mbar_init(&s_bar[s], 1);
         fence_mbar_init();
-        const uint32_t t = atomicAdd(&ctl->ticket[r], 1u);
-        s_tile[0] = t;
-        if (t < full_tiles) {
-            mbar_arrive_expect_tx(&s_bar[0], tile_bytes);
-            bulk_copy_g2s(stage_mem, src_base + (uint64_t)t * tile_bytes, tile_bytes, &s_bar[0]);
+        for (int s = 0; s < kStages - 1; s++) {
+            const uint64_t t = blockIdx.x + (uint64_t)s * gridDim.x;
+            if (t < full_tiles) {
+                mbar_arrive_expect_tx(&s_bar[s], tile_bytes);
+                bulk_copy_g2s(stage_mem + s * stage_bytes<ITEMS>(), src_base + t * tile_bytes, tile_bytes,
+                              &s_bar[s]);
+            }
         }
     }
     __syncthreads();
     uint32_t parity = 0;  // bit s: phase of stage s's barrier to wait for
-    for (uint32_t k = 0;; k++) {
-        const int s = (int)(k & 1);
-        const uint32_t t = s_tile[s];
-        if (t >= ntiles)
-            break;
+    int s = 0;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, s = (s + 1 == kStages) ? 0 : s + 1) {
         const bool bulk = t < full_tiles;
         bool ok = true;
         if (bulk) {
@@ -296,7 +329,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
         if (__syncthreads_or(!ok))
             break;  // a bulk copy never completed; the status bit is set
         const unsigned char *stage = stage_mem + s * stage_bytes<ITEMS>();
-        const uint64_t tbase = (uint64_t)t * kTileRecs;
+        const uint64_t tbase = t * kTileRecs;
         uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
         bool keep[ITEMS];
 #pragma unroll
@@ -359,15 +392,25 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
         for (int j = 0; j < ITEMS; j++) {
             keep[j] = keep[j] && ra[j] != rb[j];
             mask[j] = __ballot_sync(0xffffffffu, keep[j]);
-            // guard values travel while warp 0 scans and waits on the look-back
-            ga[j] = keep[j] ? __ldcg(a.best + ra[j]) : 0ull;
-            gb[j] = keep[j] ? __ldcg(a.best + rb[j]) : 0ull;
+            ga[j] = keep[j] ? __ldcg(&a.best[ra[j]].x) : 0ull;
+            gb[j] = keep[j] ? __ldcg(&a.best[rb[j]].x) : 0ull;
         }
         if (lane == 0)
 #pragma unroll
             for (int j = 0; j < ITEMS; j++)
                 s_cnt[j * kWarps + warp] = __popc(mask[j]);
-        __syncthreads();
+        __syncthreads();  // s_cnt complete; the stage's records are all in registers
+        if (threadIdx.x == 0) {
+            // refill this stage's slot in the ring with the tile two ahead
+            const uint64_t t2 = t + (uint64_t)(kStages - 1) * gridDim.x;
+            const int s2 = (s + kStages - 1) % kStages;
+            if (t2 < full_tiles) {
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&s_bar[s2], tile_bytes);
+                bulk_copy_g2s(stage_mem + s2 * stage_bytes<ITEMS>(), src_base + t2 * tile_bytes, tile_bytes,
+                              &s_bar[s2]);
+            }
+        }
         if (warp == 0) {
             // exclusive scan of the row/warp counts, row-major, kCnt / 32 per lane
             constexpr int kPer = kCnt / 32;
@@ -391,39 +434,24 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
                 run += c[q];
             }
             const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-            if (lane == 0) {
-                lookback_publish(a.status, t, total, epoch);
-                // next tile: ticket and bulk copy into the other stage (read last
-                // iteration, several barriers ago)
-                const uint32_t t2 = atomicAdd(&ctl->ticket[r], 1u);
-                s_tile[s ^ 1] = t2;
-                if (t2 < full_tiles) {
-                    fence_proxy_async_smem();
-                    mbar_arrive_expect_tx(&s_bar[s ^ 1], tile_bytes);
-                    bulk_copy_g2s(stage_mem + (s ^ 1) * stage_bytes<ITEMS>(), src_base + (uint64_t)t2 * tile_bytes,
-                                  tile_bytes, &s_bar[s ^ 1]);
-                }
-            }
-            __syncwarp();
-            const uint32_t ex = lookback_resolve(a.status, t, total, epoch, &ctl->err);
-            if (lane == 0) {
-                s_base = ex;
-                if (t == ntiles - 1)
-                    ctl->m_r[r] = (unsigned long long)ex + total;
-            }
+            if (lane == 31)
+                s_base = total ? (uint32_t)atomicAdd(counter, (unsigned long long)total) : 0u;
         }
-        __syncthreads();
+        // slot updates need no output position: they overlap the reservation
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const unsigned long long key = ((unsigned long long)w[j] << 32) | id[j];
+            offer_row(a.best, ra[j], key, rb[j], keep[j], ga[j], &ctl->err);
+            offer_row(a.best, rb[j], key, ra[j], keep[j], gb[j], &ctl->err);
+        }
+        __syncthreads();  // s_base and the scanned s_cnt are ready
         const uint32_t base = s_base;
         const unsigned below = (1u << lane) - 1u;
 #pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            const uint32_t pos = base + s_cnt[j * kWarps + warp] + __popc(mask[j] & below);
-            const unsigned long long key = ((unsigned long long)w[j] << 32) | pos;
+        for (int j = 0; j < ITEMS; j++)
             if (keep[j])
-                out[pos] = make_uint4(ra[j], rb[j], w[j], id[j]);
-            offer_row(a.best, ra[j], key, keep[j], ga[j]);
-            offer_row(a.best, rb[j], key, keep[j], gb[j]);
-        }
+                out[base + s_cnt[j * kWarps + warp] + __popc(mask[j] & below)] =
+                    make_uint4(ra[j], rb[j], w[j], id[j]);
         __syncthreads();  // s_cnt and s_base are free again
     }
 }
@@ -440,25 +468,18 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
     const bool all = *(volatile uint32_t *)&ctl->cand_all;
     const uint32_t count = all ? a.n : ctl->roots[r];
     const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
-    const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < count; i0 += stride) {
         const uint32_t i = i0 + threadIdx.x;
         const bool in = i < count;
         const uint32_t x = in ? (all ? i : cand[i]) : 0;
-        const unsigned long long bk = in ? a.best[x] : kKeyNone;
-        const bool active = bk != kKeyNone;
+        const ulonglong2 b = in ? a.best[x] : make_ulonglong2(kKeyNone, 0);
+        const bool active = b.x != kKeyNone;
         warp_count(&ctl->n_r[r], active);
         if (!active)
             continue;
-        const uint4 rec = wl[(uint32_t)bk];
-        const uint32_t ea = rec.x, eb = rec.y, id = rec.w;
-        if (ea != x && eb != x) {
-            set_err(&ctl->err, kErrChase);
-            continue;
-        }
-        const uint32_t other = (ea == x) ? eb : ea;
-        const bool mutual = a.best[other] == bk;
+        const uint32_t other = (uint32_t)b.y, id = (uint32_t)b.x;
+        const bool mutual = __ldcg(&a.best[other].x) == b.x;
         if (mutual && x < other)
             continue;  // stays root; the partner hooks and marks the edge
         a.parent[x] = other;
@@ -469,9 +490,10 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
 }
 
 // Pointer jumping.  Normally over this round's components only: roots that
-// remain are collected as the next round's candidates and best is reset.  In
-// the round where the light phase runs dry every vertex is compressed to its
-// root instead, so the heavy pass can relabel original endpoints in one hop.
+// remain are collected as the next round's candidates and the slots are
+// reset.  In the round where the light phase runs dry every vertex is
+// compressed to its root instead, so the heavy pass relabels original
+// endpoints in one hop.
 __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
 {
     Ctl *ctl = a.ctl;
@@ -488,7 +510,7 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
         const uint32_t i = i0 + threadIdx.x;
         const bool in = i < count;
         const uint32_t x = in ? ((all || full) ? i : cand[i]) : 0;
-        const bool active = in && (full || a.best[x] != kKeyNone);
+        const bool active = in && (full || a.best[x].x != kKeyNone);
         bool stays = false;
         if (active) {
             uint32_t y = a.parent[x];
@@ -506,7 +528,7 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
             if (a.parent[x] != y)
                 a.parent[x] = y;
             if (!full) {
-                a.best[x] = kKeyNone;
+                a.best[x] = make_ulonglong2(kKeyNone, 0);
                 stays = (y == x);
             }
         }
@@ -622,7 +644,7 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.n = p.n;
     a.epoch_base = (uint32_t)p.epoch_base;
     a.parent = p.parent;
-    a.best = p.best;
+    a.best = reinterpret_cast<ulonglong2 *>(p.best);
     a.cand0 = p.cand[0];
     a.cand1 = p.cand[1];
     a.bitmap = p.bitmap;
@@ -669,34 +691,38 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
 }
 
 template <int KIND>
+phem_status setup_kernels(phem_context *ctx)
+{
+    int per_sm = 0;
+    PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<KIND, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)pipe_smem<8>()));
+    PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<KIND, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)pipe_smem<4>()));
+    PHEM_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 8>, kBlock, pipe_smem<8>()));
+    ctx->edge_pass_blocks = ctx->sm_count * std::max(1, per_sm);
+    PHEM_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 4>, kBlock, pipe_smem<4>()));
+    ctx->edge_pass_blocks4 = ctx->sm_count * std::max(1, per_sm);
+    PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
+    ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
+    return PHEM_OK;
+}
+
+template <int KIND>
 phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
 {
     cudaStream_t s = ctx->stream;
-    if (!ctx->edge_pass_blocks) {
-        int per_sm = 0;
-        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf, 8>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<8>()));
-        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked, 8>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<8>()));
-        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindMsf, 4>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<4>()));
-        PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<kKindPacked, 4>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<4>()));
-        PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 8>, kBlock,
-                                                                    pipe_smem<8>()));
-        ctx->edge_pass_blocks = ctx->sm_count * std::max(1, per_sm);
-        PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 4>, kBlock,
-                                                                    pipe_smem<4>()));
-        ctx->edge_pass_blocks4 = ctx->sm_count * std::max(1, per_sm);
-        PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
-        ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
+    if (!(ctx->kernels_ready & (1u << KIND))) {
+        PHEM_TRY(setup_kernels<KIND>(ctx));
+        ctx->kernels_ready |= 1u << KIND;
     }
     const RoundArgs a = make_args(ctx, plan);
     // light/heavy split: about light_per_vertex * n light edges, and only when
     // the input is at least filter_min_ratio times that large
     const double lpv = ctx->tune_light_per_vertex;
     const uint64_t k = (uint64_t)(lpv * (double)plan.n);
-    const bool filter = lpv > 0 && plan.m > 0 && (double)plan.m >= ctx->tune_filter_min_ratio * (double)k;
+    const bool filter = lpv > 0 && k > 0 && (double)plan.m >= ctx->tune_filter_min_ratio * (double)k;
     unsigned long long thr = kKeyNone;
     if (filter && KIND == kKindPacked)
         thr = k;  // canonical forest: the first k edges by index are light
@@ -741,7 +767,7 @@ size_t msf_workspace_bytes(uint64_t m, uint32_t n)
 {
     Carve c;
     c.take<uint32_t>(n);
-    c.take<unsigned long long>(n);
+    c.take<ulonglong2>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>((m + 31) / 32 + 4);
@@ -763,7 +789,7 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     Carve k;
     plan->status = ctx->status;
     plan->parent = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
-    plan->best = reinterpret_cast<unsigned long long *>(base + k.take<unsigned long long>(n));
+    plan->best = reinterpret_cast<unsigned long long *>(base + k.take<ulonglong2>(n));
     plan->cand[0] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
