@@ -135,6 +135,7 @@ struct MsfPlan {
     unsigned long long *best;// n
     uint32_t *cand[2];       // n each
     uint32_t *bitmap;        // ceil(m / 32)
+    uint32_t *pos_of_id;     // m: edge id -> position in the current survivor list
     uint4 *wl[2];            // m each
     uint64_t *status;        // look-back status (context-owned), >= tiles
     uint64_t epoch_base;

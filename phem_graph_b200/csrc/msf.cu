@@ -27,11 +27,12 @@
 //      internal after the light phase closes a cycle of lighter edges, so it
 //      is in no MSF: the filter changes the work, not the result.
 //
-// Each component's choice lives in a 16-byte slot {key = w << 32 | id, the far
-// root} updated with a 128-bit compare-and-swap, so the hook step needs no
-// survivor record and the survivor list may be in any order.  That removes
-// every dependency between CTAs from the edge pass: tiles are statically
-// strided over a persistent grid, arrive in shared memory by 1-D bulk copies
+// A component's choice is the minimum key (w << 32 | id) offered to it, kept
+// with fire-and-forget 64-bit atomicMin.  The edge pass also records where it
+// wrote each survivor (pos_of_id[id]), so the hook finds the chosen record from
+// the key's id and the survivor list may be in any order.  That removes every
+// dependency between CTAs from the edge pass: tiles are statically strided
+// over a persistent grid, arrive in shared memory by 1-D bulk copies
 // (cp.async.bulk) two tiles ahead of use, and each tile reserves its output
 // range with one atomicAdd.  MSF membership is a bitmap over edge ids; one
 // ordered gather (decoupled look-back) writes the MSF records ascending by id
@@ -52,7 +53,8 @@ struct RoundArgs {
     uint32_t n;
     uint32_t epoch_base;
     uint32_t *parent;
-    ulonglong2 *best;  // per component: {key, far root}
+    unsigned long long *best;  // per component: minimum key (w << 32 | id) offered this round
+    uint32_t *pos_of_id;       // edge id -> position of its record in this round's survivor list
     uint32_t *cand0, *cand1;
     uint32_t *bitmap;
     uint4 *wl0, *wl1;
@@ -78,68 +80,30 @@ __device__ __forceinline__ unsigned long long e0_key(uint32_t w, uint64_t id)
     return KIND == kKindMsf ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
 }
 
-__device__ __forceinline__ ulonglong2 ld_cg_slot(const ulonglong2 *p)
-{
-    return __ldcg(p);
-}
-
-__device__ __forceinline__ ulonglong2 cas128(ulonglong2 *addr, ulonglong2 cmp, ulonglong2 val)
-{
-    ulonglong2 old;
-    asm volatile(
-        "{\n\t.reg .b128 c, v, o;\n\t"
-        "mov.b128 c, {%2, %3};\n\t"
-        "mov.b128 v, {%4, %5};\n\t"
-        "atom.global.cas.b128 o, [%6], c, v;\n\t"
-        "mov.b128 {%0, %1}, o;\n\t}"
-        : "=l"(old.x), "=l"(old.y)
-        : "l"(cmp.x), "l"(cmp.y), "l"(val.x), "l"(val.y), "l"(addr)
-        : "memory");
-    return old;
-}
-
-constexpr uint32_t kCasCap = 1u << 16;
-
-// Lowers slot t to {key, far} if key is smaller.  `guard` is an earlier read
-// of the slot's key: it may be stale but never below the true one, so it only
-// skips updates that could not win.
-__device__ __forceinline__ void slot_min(ulonglong2 *best, uint32_t t, unsigned long long key, uint32_t far,
-                                         unsigned long long guard, uint32_t *err)
-{
-    if (key >= guard)
-        return;
-    ulonglong2 cur = ld_cg_slot(best + t);
-    const ulonglong2 mine = make_ulonglong2(key, far);
-    for (uint32_t i = 0; i < kCasCap; i++) {
-        if (key >= cur.x)
-            return;
-        const ulonglong2 old = cas128(best + t, cur, mine);
-        if (old.x == cur.x && old.y == cur.y)
-            return;
-        cur = old;
-    }
-    set_err(err, kErrRetry);
-}
-
-// Offers edge (key, far) to slot t for the live lanes of a warp.  When every
-// live lane has the same target (a hub's run in row-major input) the warp
-// reduces the key first and only the winning lane updates the slot.
-__device__ __forceinline__ void offer_row(ulonglong2 *best, uint32_t t, unsigned long long key, uint32_t far,
-                                          bool live, unsigned long long guard, uint32_t *err)
+// Offers key to best[t] for the live lanes of a warp with a fire-and-forget
+// 64-bit atomicMin.  `guard` is an earlier read of best[t]: it may be stale but
+// never below the true value, so it only skips updates that could not win.
+// When every live lane has the same target (a hub's run in row-major input)
+// the warp reduces the key first (high word, then low word among the lanes
+// holding the minimum high word) and one lane does the atomic.
+__device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, unsigned long long key, bool live,
+                                          unsigned long long guard)
 {
     const unsigned act = __ballot_sync(0xffffffffu, live);
     if (!act)
         return;
-    const uint32_t t0 = __shfl_sync(0xffffffffu, t, __ffs(act) - 1);
+    const int leader = __ffs(act) - 1;
+    const uint32_t t0 = __shfl_sync(0xffffffffu, t, leader);
     if (__all_sync(0xffffffffu, !live || t == t0)) {
         const uint32_t hi = live ? (uint32_t)(key >> 32) : 0xffffffffu;
         const uint32_t lo = live ? (uint32_t)key : 0xffffffffu;
         const uint32_t mhi = __reduce_min_sync(0xffffffffu, hi);
         const uint32_t mlo = __reduce_min_sync(0xffffffffu, hi == mhi ? lo : 0xffffffffu);
-        if (live && hi == mhi && lo == mlo)  // keys are unique: exactly one lane
-            slot_min(best, t, key, far, guard, err);
-    } else if (live) {
-        slot_min(best, t, key, far, guard, err);
+        const unsigned long long km = ((unsigned long long)mhi << 32) | mlo;
+        if ((int)lane_id() == leader && km < guard)
+            atomicMin(best + t0, km);
+    } else if (live && key < guard) {
+        atomicMin(best + t, key);
     }
 }
 
@@ -173,7 +137,7 @@ __global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a, unsigned long
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.n; x += stride) {
         a.parent[x] = x;
-        a.best[x] = make_ulonglong2(kKeyNone, 0);
+        a.best[x] = kKeyNone;
         if (a.forest)
             a.forest[x] = kForestEmpty;
     }
@@ -392,8 +356,8 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         for (int j = 0; j < ITEMS; j++) {
             keep[j] = keep[j] && ra[j] != rb[j];
             mask[j] = __ballot_sync(0xffffffffu, keep[j]);
-            ga[j] = keep[j] ? __ldcg(&a.best[ra[j]].x) : 0ull;
-            gb[j] = keep[j] ? __ldcg(&a.best[rb[j]].x) : 0ull;
+            ga[j] = keep[j] ? __ldcg(a.best + ra[j]) : 0ull;
+            gb[j] = keep[j] ? __ldcg(a.best + rb[j]) : 0ull;
         }
         if (lane == 0)
 #pragma unroll
@@ -437,21 +401,23 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             if (lane == 31)
                 s_base = total ? (uint32_t)atomicAdd(counter, (unsigned long long)total) : 0u;
         }
-        // slot updates need no output position: they overlap the reservation
+        // offers need no output position: they overlap the reservation
 #pragma unroll
         for (int j = 0; j < ITEMS; j++) {
             const unsigned long long key = ((unsigned long long)w[j] << 32) | id[j];
-            offer_row(a.best, ra[j], key, rb[j], keep[j], ga[j], &ctl->err);
-            offer_row(a.best, rb[j], key, ra[j], keep[j], gb[j], &ctl->err);
+            offer_row(a.best, ra[j], key, keep[j], ga[j]);
+            offer_row(a.best, rb[j], key, keep[j], gb[j]);
         }
         __syncthreads();  // s_base and the scanned s_cnt are ready
         const uint32_t base = s_base;
         const unsigned below = (1u << lane) - 1u;
 #pragma unroll
         for (int j = 0; j < ITEMS; j++)
-            if (keep[j])
-                out[base + s_cnt[j * kWarps + warp] + __popc(mask[j] & below)] =
-                    make_uint4(ra[j], rb[j], w[j], id[j]);
+            if (keep[j]) {
+                const uint32_t pos = base + s_cnt[j * kWarps + warp] + __popc(mask[j] & below);
+                out[pos] = make_uint4(ra[j], rb[j], w[j], id[j]);
+                a.pos_of_id[id[j]] = pos;
+            }
         __syncthreads();  // s_cnt and s_base are free again
     }
 }
@@ -468,18 +434,25 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
     const bool all = *(volatile uint32_t *)&ctl->cand_all;
     const uint32_t count = all ? a.n : ctl->roots[r];
     const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
+    const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < count; i0 += stride) {
         const uint32_t i = i0 + threadIdx.x;
         const bool in = i < count;
         const uint32_t x = in ? (all ? i : cand[i]) : 0;
-        const ulonglong2 b = in ? a.best[x] : make_ulonglong2(kKeyNone, 0);
-        const bool active = b.x != kKeyNone;
+        const unsigned long long bk = in ? a.best[x] : kKeyNone;
+        const bool active = bk != kKeyNone;
         warp_count(&ctl->n_r[r], active);
         if (!active)
             continue;
-        const uint32_t other = (uint32_t)b.y, id = (uint32_t)b.x;
-        const bool mutual = __ldcg(&a.best[other].x) == b.x;
+        const uint32_t id = (uint32_t)bk;
+        const uint4 rec = wl[a.pos_of_id[id]];  // the chosen edge, relabelled to this round's roots
+        if (rec.x != x && rec.y != x) {
+            set_err(&ctl->err, kErrChase);
+            continue;
+        }
+        const uint32_t other = rec.x == x ? rec.y : rec.x;
+        const bool mutual = a.best[other] == bk;
         if (mutual && x < other)
             continue;  // stays root; the partner hooks and marks the edge
         a.parent[x] = other;
@@ -510,7 +483,7 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
         const uint32_t i = i0 + threadIdx.x;
         const bool in = i < count;
         const uint32_t x = in ? ((all || full) ? i : cand[i]) : 0;
-        const bool active = in && (full || a.best[x].x != kKeyNone);
+        const bool active = in && (full || a.best[x] != kKeyNone);
         bool stays = false;
         if (active) {
             uint32_t y = a.parent[x];
@@ -528,7 +501,7 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
             if (a.parent[x] != y)
                 a.parent[x] = y;
             if (!full) {
-                a.best[x] = make_ulonglong2(kKeyNone, 0);
+                a.best[x] = kKeyNone;
                 stays = (y == x);
             }
         }
@@ -644,7 +617,8 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.n = p.n;
     a.epoch_base = (uint32_t)p.epoch_base;
     a.parent = p.parent;
-    a.best = reinterpret_cast<ulonglong2 *>(p.best);
+    a.best = p.best;
+    a.pos_of_id = p.pos_of_id;
     a.cand0 = p.cand[0];
     a.cand1 = p.cand[1];
     a.bitmap = p.bitmap;
@@ -763,14 +737,18 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
 
 }  // namespace
 
+// Workspace of one solve: parent (4n), best (8n), two candidate lists (4n
+// each), the MSF bitmap (m / 8), edge id -> survivor position (4m) and two
+// survivor lists (16m each).  The carve order is fixed; msf_plan repeats it.
 size_t msf_workspace_bytes(uint64_t m, uint32_t n)
 {
     Carve c;
     c.take<uint32_t>(n);
-    c.take<ulonglong2>(n);
+    c.take<unsigned long long>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>((m + 31) / 32 + 4);
+    c.take<uint32_t>(m);
     c.take<uint4>(m);
     c.take<uint4>(m);
     return c.off;
@@ -789,10 +767,11 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     Carve k;
     plan->status = ctx->status;
     plan->parent = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
-    plan->best = reinterpret_cast<unsigned long long *>(base + k.take<ulonglong2>(n));
+    plan->best = reinterpret_cast<unsigned long long *>(base + k.take<unsigned long long>(n));
     plan->cand[0] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
+    plan->pos_of_id = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(m));
     plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(m));
     plan->wl[1] = reinterpret_cast<uint4 *>(base + k.take<uint4>(m));
     plan->e0 = d_e0;
