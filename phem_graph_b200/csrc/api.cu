@@ -289,6 +289,10 @@ phem_status copy_back(phem_context *ctx, const Staged &st, size_t bytes)
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Edge ids and survivor-list positions are 32-bit; a survivor list holds the
+// edges plus up to 2^24 records of padding.
+constexpr uint64_t kMaxEdges = (1ull << 32) - (1ull << 24);
+
 }  // namespace
 }  // namespace phem
 
@@ -544,8 +548,8 @@ phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, i
         return PHEM_ERR_INVALID;
     }
     const bool canonical = flags & PHEM_CC_CANONICAL;
-    if (canonical && (uint64_t)m >= (1ull << 32)) {
-        set_error("cc_solve: canonical forest needs m < 2^32");
+    if (canonical && (uint64_t)m > kMaxEdges) {
+        set_error("cc_solve: canonical forest needs m <= 2^32 - 2^24");
         return PHEM_ERR_INVALID;
     }
     DeviceGuard g(ctx->device);
@@ -723,8 +727,8 @@ phem_status phem_cc_merge(phem_context *ctx, const uint64_t *d_forest_a, const u
 static phem_status msf_common(phem_context *ctx, const phem_edge *edges, uint64_t m, uint32_t n, phem_edge *msf,
                               uint64_t *count, uint64_t *total, phem_msf_stats *stats, uint64_t *d_count_total)
 {
-    if (n == 0 || n == UINT32_MAX || m >= (1ull << 32) || (m > 0 && !edges)) {
-        set_error("msf: need 0 < n < 2^32 - 1, m < 2^32 and an edge array");
+    if (n == 0 || n == UINT32_MAX || m > kMaxEdges || (m > 0 && !edges)) {
+        set_error("msf: need 0 < n < 2^32 - 1, m <= 2^32 - 2^24 and an edge array");
         return PHEM_ERR_INVALID;
     }
     const size_t eb = (size_t)m * sizeof(phem_edge), ob = (size_t)n * sizeof(phem_edge);

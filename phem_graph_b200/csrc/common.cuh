@@ -41,7 +41,9 @@ struct Ctl {
     uint32_t light_rounds;                           // rounds spent in the light phase
     uint32_t pad0;
     unsigned long long threshold;                    // light edge <=> key < threshold
-    unsigned long long m_r[PHEM_MAX_ROUNDS + 1];     // live edges entering round r
+    unsigned long long m_r[PHEM_MAX_ROUNDS + 1];     // live edges entering round r (exact)
+    unsigned long long wl_len[PHEM_MAX_ROUNDS + 1];  // records written by round r's edge pass,
+                                                     // including dead padding at chunk tails
     unsigned long long n_r[PHEM_MAX_ROUNDS + 1];     // components with a live edge in round r
     uint32_t roots[PHEM_MAX_ROUNDS + 2];             // |candidate roots| entering round r
     uint32_t ticket[PHEM_MAX_ROUNDS + 2];            // tile tickets of the round's edge pass

@@ -142,7 +142,7 @@ struct MsfPlan {
     uint64_t *forest;        // kKindPacked only: forest slot per hooked root (may be null)
 };
 
-size_t msf_workspace_bytes(uint64_t m, uint32_t n);
+size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count);
 phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, uint32_t n, size_t extra_bytes,
                      MsfPlan *plan, size_t *extra_off);
 // Queues the whole Boruvka solve; returns after the rounds are done (host

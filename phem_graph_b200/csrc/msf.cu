@@ -228,6 +228,8 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
 // with one atomicAdd on the round's counter while every warp is already
 // updating component slots.
 constexpr int kStages = 3;
+constexpr unsigned long long kChunk = 4096;  // output records reserved per atomicAdd
+constexpr uint64_t kMaxEdgeCtasPerSm = 4;      // edge-pass grid bound (sizes the list padding)
 
 template <int ITEMS>
 __host__ __device__ constexpr size_t stage_bytes()
@@ -248,7 +250,8 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     extern __shared__ __align__(128) unsigned char stage_mem[];
     __shared__ uint64_t s_bar[kStages];
     __shared__ uint32_t s_cnt[kCnt];
-    __shared__ uint32_t s_base;
+    __shared__ unsigned long long s_base, s_base2;
+    __shared__ uint32_t s_split;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     const uint32_t src = *(volatile uint32_t *)&ctl->src;
     const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
     const bool from_e0 = src != kSrcList;
-    const uint64_t count = from_e0 ? a.m : ctl->m_r[r - 1];
+    const uint64_t count = from_e0 ? a.m : ctl->wl_len[r - 1];
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
     uint4 *out = (r & 1) ? a.wl1 : a.wl0;       // WL[r & 1]
     const uint32_t rec_bytes = from_e0 ? (KIND == kKindMsf ? 12u : 8u) : 16u;
@@ -265,7 +268,13 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     const uint64_t ntiles = (count + kTileRecs - 1) / kTileRecs;
     const uint64_t full_tiles = count / kTileRecs;  // the partial last tile is read directly
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    unsigned long long *counter = &ctl->m_r[r];
+    // Output space is reserved in chunks of up to kChunk records per CTA (one
+    // atomicAdd per chunk, not per tile); a tile that does not fit finishes the
+    // current chunk and continues in the next.  The unused tail of the CTA's
+    // last chunk is filled with dead records {0, 0, 0, 0}, which the next pass
+    // drops (equal roots), so a list holds at most one chunk of padding per CTA.
+    // Owned by lane 31 of warp 0: chunk cursor, room left, survivors written.
+    unsigned long long chunk_next = 0, chunk_left = 0, live = 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++)
@@ -319,14 +328,14 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                     u = (uint32_t)(e >> 32);
                     v = (uint32_t)e;
                 }
-                bool live = inb && e0_live<KIND>(u, v);
-                if (live && (u >= a.n || v >= a.n)) {
+                bool ok_e = inb && e0_live<KIND>(u, v);
+                if (ok_e && (u >= a.n || v >= a.n)) {
                     if (src == kSrcLight)
                         set_err(&ctl->err, kErrRange);
-                    live = false;
+                    ok_e = false;
                 }
                 const bool light = e0_key<KIND>(ww, gi) < thr;
-                keep[j] = live && (src == kSrcLight ? light : !light);
+                keep[j] = ok_e && (src == kSrcLight ? light : !light);
                 ra[j] = u;
                 rb[j] = v;
                 w[j] = ww;
@@ -365,7 +374,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                 s_cnt[j * kWarps + warp] = __popc(mask[j]);
         __syncthreads();  // s_cnt complete; the stage's records are all in registers
         if (threadIdx.x == 0) {
-            // refill this stage's slot in the ring with the tile two ahead
+            // refill the stage read last iteration with the tile two ahead
             const uint64_t t2 = t + (uint64_t)(kStages - 1) * gridDim.x;
             const int s2 = (s + kStages - 1) % kStages;
             if (t2 < full_tiles) {
@@ -397,9 +406,29 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                 s_cnt[kPer * lane + q] = run;
                 run += c[q];
             }
-            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-            if (lane == 31)
-                s_base = total ? (uint32_t)atomicAdd(counter, (unsigned long long)total) : 0u;
+            if (lane == 31) {
+                const unsigned long long total = incl;
+                s_base = chunk_next;
+                if (total <= chunk_left) {
+                    s_split = (uint32_t)total;
+                    chunk_next += total;
+                    chunk_left -= total;
+                } else {
+                    // the first chunk_left survivors finish the current chunk, the
+                    // rest open a new one sized to this CTA's remaining input
+                    s_split = (uint32_t)chunk_left;
+                    const unsigned long long rest = total - chunk_left;
+                    const uint64_t tiles_left = (ntiles - 1 - t) / gridDim.x + 1;
+                    const unsigned long long cap = tiles_left * kTileRecs;
+                    const unsigned long long want = cap < kChunk ? cap : kChunk;
+                    const unsigned long long size = want > rest ? want : rest;
+                    const unsigned long long fresh = atomicAdd(&ctl->wl_len[r], size);
+                    s_base2 = fresh;
+                    chunk_next = fresh + rest;
+                    chunk_left = size - rest;
+                }
+                live += total;
+            }
         }
         // offers need no output position: they overlap the reservation
 #pragma unroll
@@ -408,110 +437,180 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             offer_row(a.best, ra[j], key, keep[j], ga[j]);
             offer_row(a.best, rb[j], key, keep[j], gb[j]);
         }
-        __syncthreads();  // s_base and the scanned s_cnt are ready
-        const uint32_t base = s_base;
+        __syncthreads();  // s_base, s_base2, s_split and the scanned s_cnt are ready
+        const unsigned long long base = s_base, base2 = s_base2;
+        const uint32_t split = s_split;
         const unsigned below = (1u << lane) - 1u;
 #pragma unroll
         for (int j = 0; j < ITEMS; j++)
             if (keep[j]) {
-                const uint32_t pos = base + s_cnt[j * kWarps + warp] + __popc(mask[j] & below);
+                const uint32_t rank = s_cnt[j * kWarps + warp] + __popc(mask[j] & below);
+                const unsigned long long pos = rank < split ? base + rank : base2 + (rank - split);
                 out[pos] = make_uint4(ra[j], rb[j], w[j], id[j]);
-                a.pos_of_id[id[j]] = pos;
+                a.pos_of_id[id[j]] = (uint32_t)pos;
             }
-        __syncthreads();  // s_cnt and s_base are free again
+        __syncthreads();  // s_cnt and the bases are free again
     }
+    // pad the last chunk's unused tail with dead records and publish this
+    // CTA's exact survivor count
+    if (threadIdx.x == 31) {
+        s_base = chunk_next;
+        s_split = (uint32_t)chunk_left;
+        if (live)
+            atomicAdd(&ctl->m_r[r], live);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < s_split; i += kBlock)
+        out[s_base + i] = make_uint4(0, 0, 0, 0);
 }
 
 // Hook: each component that found an edge either stays root (lower id of a
-// mutual pair) or points at the far component and marks its edge.
+// mutual pair) or points at the far component and marks its edge.  kVItems
+// candidates per thread per iteration keep several dependent chains in flight.
+constexpr int kVItems = 4;
+
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
 {
+    __shared__ unsigned long long s_red[kWarps];
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const bool all = *(volatile uint32_t *)&ctl->cand_all;
-    const uint32_t count = all ? a.n : ctl->roots[r];
+    const uint64_t count = all ? a.n : ctl->roots[r];
     const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
     const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < count; i0 += stride) {
-        const uint32_t i = i0 + threadIdx.x;
-        const bool in = i < count;
-        const uint32_t x = in ? (all ? i : cand[i]) : 0;
-        const unsigned long long bk = in ? a.best[x] : kKeyNone;
-        const bool active = bk != kKeyNone;
-        warp_count(&ctl->n_r[r], active);
-        if (!active)
-            continue;
-        const uint32_t id = (uint32_t)bk;
-        const uint4 rec = wl[a.pos_of_id[id]];  // the chosen edge, relabelled to this round's roots
-        if (rec.x != x && rec.y != x) {
-            set_err(&ctl->err, kErrChase);
-            continue;
+    unsigned long long active_cnt = 0;
+    const uint64_t step = (uint64_t)gridDim.x * kBlock * kVItems;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * kVItems; i0 < count; i0 += step) {
+        uint32_t x[kVItems];
+        unsigned long long bk[kVItems];
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
+            const uint64_t i = i0 + k * kBlock + threadIdx.x;
+            x[k] = i < count ? (all ? (uint32_t)i : cand[i]) : 0;
+            bk[k] = i < count ? a.best[x[k]] : kKeyNone;
         }
-        const uint32_t other = rec.x == x ? rec.y : rec.x;
-        const bool mutual = a.best[other] == bk;
-        if (mutual && x < other)
-            continue;  // stays root; the partner hooks and marks the edge
-        a.parent[x] = other;
-        atomicOr(a.bitmap + (id >> 5), 1u << (id & 31));
-        if (KIND == kKindPacked && a.forest)
-            a.forest[x] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
+        uint32_t pos[kVItems];
+#pragma unroll
+        for (int k = 0; k < kVItems; k++)
+            pos[k] = bk[k] != kKeyNone ? a.pos_of_id[(uint32_t)bk[k]] : 0;
+        uint4 rec[kVItems];
+#pragma unroll
+        for (int k = 0; k < kVItems; k++)
+            rec[k] = bk[k] != kKeyNone ? wl[pos[k]] : make_uint4(0, 0, 0, 0);
+        uint32_t other[kVItems];
+        unsigned long long ob[kVItems];
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
+            other[k] = rec[k].x == x[k] ? rec[k].y : rec[k].x;
+            ob[k] = bk[k] != kKeyNone ? __ldcg(a.best + other[k]) : 0ull;
+        }
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
+            if (bk[k] == kKeyNone)
+                continue;
+            active_cnt++;
+            const uint32_t id = (uint32_t)bk[k];
+            if (rec[k].x != x[k] && rec[k].y != x[k]) {
+                set_err(&ctl->err, kErrChase);
+                continue;
+            }
+            if (ob[k] == bk[k] && x[k] < other[k])
+                continue;  // mutual pair: the lower id stays root, the partner hooks
+            a.parent[x[k]] = other[k];
+            atomicOr(a.bitmap + (id >> 5), 1u << (id & 31));
+            if (KIND == kKindPacked && a.forest)
+                a.forest[x[k]] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
+        }
     }
+    const unsigned long long tot = block_sum_u64(active_cnt, s_red);
+    if (threadIdx.x == 0 && tot)
+        atomicAdd(&ctl->n_r[r], tot);
 }
 
 // Pointer jumping.  Normally over this round's components only: roots that
-// remain are collected as the next round's candidates and the slots are
-// reset.  In the round where the light phase runs dry every vertex is
-// compressed to its root instead, so the heavy pass relabels original
-// endpoints in one hop.
+// remain are collected as the next round's candidates (one atomicAdd per
+// block-iteration) and best is reset.  In the round where the light phase runs
+// dry every vertex is compressed to its root instead, so the heavy pass
+// relabels original endpoints in one hop.
 __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
 {
+    __shared__ uint32_t s_warp[kWarps];
+    __shared__ uint32_t s_base;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const bool all = *(volatile uint32_t *)&ctl->cand_all;
     const bool full = *(volatile uint32_t *)&ctl->phase == 0 && ctl->m_r[r] == 0;
-    const uint32_t count = (all || full) ? a.n : ctl->roots[r];
+    const uint64_t count = (all || full) ? a.n : ctl->roots[r];
     const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
     uint32_t *next = (r & 1) ? a.cand0 : a.cand1;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < count; i0 += stride) {
-        const uint32_t i = i0 + threadIdx.x;
-        const bool in = i < count;
-        const uint32_t x = in ? ((all || full) ? i : cand[i]) : 0;
-        const bool active = in && (full || a.best[x] != kKeyNone);
-        bool stays = false;
-        if (active) {
-            uint32_t y = a.parent[x];
-            uint32_t steps = 0;
-            for (;;) {
-                const uint32_t p = a.parent[y];
-                if (p == y)
-                    break;
-                y = p;
-                if (++steps > a.n) {
-                    set_err(&ctl->err, kErrChase);
-                    break;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint64_t step = (uint64_t)gridDim.x * kBlock * kVItems;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * kVItems; i0 < count; i0 += step) {
+        bool stays[kVItems];
+        uint32_t x[kVItems];
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
+            const uint64_t i = i0 + k * kBlock + threadIdx.x;
+            const bool in = i < count;
+            x[k] = in ? ((all || full) ? (uint32_t)i : cand[i]) : 0;
+            const bool active = in && (full || a.best[x[k]] != kKeyNone);
+            stays[k] = false;
+            if (active) {
+                uint32_t y = a.parent[x[k]];
+                uint32_t steps = 0;
+                for (;;) {
+                    const uint32_t p = a.parent[y];
+                    if (p == y)
+                        break;
+                    y = p;
+                    if (++steps > a.n) {
+                        set_err(&ctl->err, kErrChase);
+                        break;
+                    }
+                }
+                if (a.parent[x[k]] != y)
+                    a.parent[x[k]] = y;
+                if (!full) {
+                    a.best[x[k]] = kKeyNone;
+                    stays[k] = (y == x[k]);
                 }
             }
-            if (a.parent[x] != y)
-                a.parent[x] = y;
-            if (!full) {
-                a.best[x] = kKeyNone;
-                stays = (y == x);
-            }
         }
-        const unsigned b = __ballot_sync(0xffffffffu, stays);
-        uint32_t slot = 0;
-        if (lane_id() == 0 && b)
-            slot = atomicAdd(&ctl->roots[r + 1], (uint32_t)__popc(b));
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        if (stays)
-            next[slot + __popc(b & ((1u << lane_id()) - 1))] = x;
+        if (full)
+            continue;  // uniform: no candidate list in the compress-all round
+        unsigned m[kVItems];
+        uint32_t wsum = 0;
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
+            m[k] = __ballot_sync(0xffffffffu, stays[k]);
+            wsum += __popc(m[k]);
+        }
+        if (lane == 0)
+            s_warp[warp] = wsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t tot = 0;
+            for (int q = 0; q < kWarps; q++) {
+                const uint32_t c = s_warp[q];
+                s_warp[q] = tot;
+                tot += c;
+            }
+            s_base = tot ? atomicAdd(&ctl->roots[r + 1], tot) : 0u;
+        }
+        __syncthreads();
+        uint32_t pos = s_base + s_warp[warp];
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
+            if (stays[k])
+                next[pos + __popc(m[k] & ((1u << lane) - 1))] = x[k];
+            pos += __popc(m[k]);
+        }
+        __syncthreads();  // s_warp / s_base reused next iteration
     }
 }
 
@@ -674,10 +773,10 @@ phem_status setup_kernels(phem_context *ctx)
                                        (int)pipe_smem<4>()));
     PHEM_CUDA_TRY(
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 8>, kBlock, pipe_smem<8>()));
-    ctx->edge_pass_blocks = ctx->sm_count * std::max(1, per_sm);
+    ctx->edge_pass_blocks = ctx->sm_count * std::max(1, std::min(per_sm, (int)kMaxEdgeCtasPerSm));
     PHEM_CUDA_TRY(
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 4>, kBlock, pipe_smem<4>()));
-    ctx->edge_pass_blocks4 = ctx->sm_count * std::max(1, per_sm);
+    ctx->edge_pass_blocks4 = ctx->sm_count * std::max(1, std::min(per_sm, (int)kMaxEdgeCtasPerSm));
     PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
     ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
     return PHEM_OK;
@@ -737,10 +836,15 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
 
 }  // namespace
 
+// Records a survivor list may need: every edge plus one chunk of dead padding
+// per edge-pass CTA (at most kMaxEdgeCtasPerSm per SM).
+uint64_t wl_capacity(uint64_t m, int sm_count) { return m + (uint64_t)sm_count * kMaxEdgeCtasPerSm * kChunk; }
+
 // Workspace of one solve: parent (4n), best (8n), two candidate lists (4n
 // each), the MSF bitmap (m / 8), edge id -> survivor position (4m) and two
-// survivor lists (16m each).  The carve order is fixed; msf_plan repeats it.
-size_t msf_workspace_bytes(uint64_t m, uint32_t n)
+// survivor lists (16 bytes per record each).  The carve order is fixed;
+// msf_plan repeats it.
+size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
 {
     Carve c;
     c.take<uint32_t>(n);
@@ -749,15 +853,15 @@ size_t msf_workspace_bytes(uint64_t m, uint32_t n)
     c.take<uint32_t>(n);
     c.take<uint32_t>((m + 31) / 32 + 4);
     c.take<uint32_t>(m);
-    c.take<uint4>(m);
-    c.take<uint4>(m);
+    c.take<uint4>(wl_capacity(m, sm_count));
+    c.take<uint4>(wl_capacity(m, sm_count));
     return c.off;
 }
 
 phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, uint32_t n, size_t extra_bytes,
                      MsfPlan *plan, size_t *extra_off)
 {
-    const size_t core = msf_workspace_bytes(m, n);
+    const size_t core = msf_workspace_bytes(m, n, ctx->sm_count);
     Carve c;
     c.off = core;
     const size_t extra_at = c.take<uint8_t>(extra_bytes);
@@ -772,8 +876,8 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
     plan->pos_of_id = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(m));
-    plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(m));
-    plan->wl[1] = reinterpret_cast<uint4 *>(base + k.take<uint4>(m));
+    plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
+    plan->wl[1] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->e0 = d_e0;
     plan->m = m;
     plan->n = n;
