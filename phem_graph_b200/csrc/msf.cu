@@ -28,13 +28,14 @@
 //      is in no MSF: the filter changes the work, not the result.
 //
 // A component's choice is the minimum key (w << 32 | id) offered to it, kept
-// with fire-and-forget 64-bit atomicMin.  The edge pass also records where it
-// wrote each survivor (pos_of_id[id]), so the hook finds the chosen record from
-// the key's id and the survivor list may be in any order.  That removes every
-// dependency between CTAs from the edge pass: tiles are statically strided
-// over a persistent grid, arrive in shared memory by 1-D bulk copies
-// (cp.async.bulk) two tiles ahead of use, and each tile reserves its output
-// range with one atomicAdd.  MSF membership is a bitmap over edge ids; one
+// with fire-and-forget 64-bit atomicMin.  A short record-parallel resolve pass
+// then stores, for each component, the far root of the survivor whose key won
+// there, so the hook needs no survivor record and the survivor list may be in
+// any order.  That removes every dependency between CTAs from the edge pass:
+// tiles are statically strided over a persistent grid, arrive in shared memory
+// by 1-D bulk copies (cp.async.bulk) two tiles ahead of use, survivors are
+// staged densely in shared memory before their coalesced write, and output
+// space is reserved in chunks with one atomicAdd each.  MSF membership is a bitmap over edge ids; one
 // ordered gather (decoupled look-back) writes the MSF records ascending by id
 // with the uint64 total.  Every round kernel reads the round, phase and
 // continue flag from the device control block, so rounds are queued ahead
@@ -54,7 +55,7 @@ struct RoundArgs {
     uint32_t epoch_base;
     uint32_t *parent;
     unsigned long long *best;  // per component: minimum key (w << 32 | id) offered this round
-    uint32_t *pos_of_id;       // edge id -> position of its record in this round's survivor list
+    uint32_t *far;             // per component: far root of the edge it chose (set by resolve)
     uint32_t *cand0, *cand1;
     uint32_t *bitmap;
     uint4 *wl0, *wl1;
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     __shared__ uint64_t s_bar[kStages];
     __shared__ uint32_t s_cnt[kCnt];
     __shared__ unsigned long long s_base, s_base2;
-    __shared__ uint32_t s_split;
+    __shared__ uint32_t s_split, s_total;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         }
         if (__syncthreads_or(!ok))
             break;  // a bulk copy never completed; the status bit is set
-        const unsigned char *stage = stage_mem + s * stage_bytes<ITEMS>();
+        unsigned char *stage = stage_mem + s * stage_bytes<ITEMS>();
         const uint64_t tbase = t * kTileRecs;
         uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
         bool keep[ITEMS];
@@ -360,19 +361,16 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                 }
         }
         unsigned mask[ITEMS];
-        unsigned long long ga[ITEMS], gb[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; j++) {
             keep[j] = keep[j] && ra[j] != rb[j];
             mask[j] = __ballot_sync(0xffffffffu, keep[j]);
-            ga[j] = keep[j] ? __ldcg(a.best + ra[j]) : 0ull;
-            gb[j] = keep[j] ? __ldcg(a.best + rb[j]) : 0ull;
         }
         if (lane == 0)
 #pragma unroll
             for (int j = 0; j < ITEMS; j++)
                 s_cnt[j * kWarps + warp] = __popc(mask[j]);
-        __syncthreads();  // s_cnt complete; the stage's records are all in registers
+        __syncthreads();  // s_cnt complete; every record of the stage is in registers
         if (threadIdx.x == 0) {
             // refill the stage read last iteration with the tile two ahead
             const uint64_t t2 = t + (uint64_t)(kStages - 1) * gridDim.x;
@@ -408,6 +406,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             }
             if (lane == 31) {
                 const unsigned long long total = incl;
+                s_total = (uint32_t)total;
                 s_base = chunk_next;
                 if (total <= chunk_left) {
                     s_split = (uint32_t)total;
@@ -430,26 +429,47 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                 live += total;
             }
         }
-        // offers need no output position: they overlap the reservation
-#pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            const unsigned long long key = ((unsigned long long)w[j] << 32) | id[j];
-            offer_row(a.best, ra[j], key, keep[j], ga[j]);
-            offer_row(a.best, rb[j], key, keep[j], gb[j]);
-        }
-        __syncthreads();  // s_base, s_base2, s_split and the scanned s_cnt are ready
-        const unsigned long long base = s_base, base2 = s_base2;
-        const uint32_t split = s_split;
+        __syncthreads();  // ranks, bases and split are ready
+        // Stage the survivors densely, in rank (= input) order, in this
+        // tile's own stage buffer: its input is already in registers, and the
+        // buffer is refilled only after this tile's last barrier.
+        uint4 *staging = reinterpret_cast<uint4 *>(stage);
         const unsigned below = (1u << lane) - 1u;
 #pragma unroll
         for (int j = 0; j < ITEMS; j++)
-            if (keep[j]) {
-                const uint32_t rank = s_cnt[j * kWarps + warp] + __popc(mask[j] & below);
-                const unsigned long long pos = rank < split ? base + rank : base2 + (rank - split);
-                out[pos] = make_uint4(ra[j], rb[j], w[j], id[j]);
-                a.pos_of_id[id[j]] = (uint32_t)pos;
+            if (keep[j])
+                staging[s_cnt[j * kWarps + warp] + __popc(mask[j] & below)] = make_uint4(ra[j], rb[j], w[j], id[j]);
+        __syncthreads();
+        // Dense phase: coalesced survivor writes and the offers of both
+        // endpoints, several records per thread so the guard loads overlap.
+        const uint32_t total = s_total, split = s_split;
+        const unsigned long long base = s_base, base2 = s_base2;
+        for (uint32_t i0 = 0; i0 < total; i0 += kBlock * 4) {
+            uint4 rec[4];
+            bool on[4];
+            unsigned long long key[4], ga[4], gb[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t i = i0 + q * kBlock + threadIdx.x;
+                on[q] = i < total;
+                rec[q] = on[q] ? staging[i] : make_uint4(0, 0, 0, 0);
+                key[q] = ((unsigned long long)rec[q].z << 32) | rec[q].w;
+                ga[q] = on[q] ? __ldcg(a.best + rec[q].x) : 0ull;
+                gb[q] = on[q] ? __ldcg(a.best + rec[q].y) : 0ull;
             }
-        __syncthreads();  // s_cnt and the bases are free again
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t i = i0 + q * kBlock + threadIdx.x;
+                if (on[q])
+                    out[i < split ? base + i : base2 + (i - split)] = rec[q];
+                offer_row(a.best, rec[q].x, key[q], on[q], ga[q]);
+                offer_row(a.best, rec[q].y, key[q], on[q], gb[q]);
+            }
+        }
+        // this thread's staging writes and reads of the stage come before the
+        // bulk copy that will refill it
+        fence_proxy_async_smem();
+        __syncthreads();  // staging, s_cnt and the bases are free again
     }
     // pad the last chunk's unused tail with dead records and publish this
     // CTA's exact survivor count
@@ -462,6 +482,43 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < s_split; i += kBlock)
         out[s_base + i] = make_uint4(0, 0, 0, 0);
+}
+
+// Resolve: for every survivor of this round whose key won at an endpoint's
+// component, record the far component there.  Keys are unique, so exactly
+// one record writes each far[x].  Dead padding records (equal roots) are
+// skipped.  The list was just written, so it is mostly read from L2.
+__global__ void __launch_bounds__(kBlock) resolve_kernel(RoundArgs a)
+{
+    Ctl *ctl = a.ctl;
+    if (!*(volatile uint32_t *)&ctl->go)
+        return;
+    const uint32_t r = *(volatile uint32_t *)&ctl->round;
+    const uint64_t len = ctl->wl_len[r];
+    const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
+    const uint64_t step = (uint64_t)gridDim.x * kBlock * 4;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * 4; i0 < len; i0 += step) {
+        uint4 rec[4];
+        unsigned long long ka[4], kb[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint64_t i = i0 + q * kBlock + threadIdx.x;
+            rec[q] = i < len ? __ldcg(wl + i) : make_uint4(0, 0, 0, 0);
+            const bool real = rec[q].x != rec[q].y;
+            ka[q] = real ? __ldcg(a.best + rec[q].x) : 0ull;
+            kb[q] = real ? __ldcg(a.best + rec[q].y) : 0ull;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (rec[q].x == rec[q].y)
+                continue;
+            const unsigned long long key = ((unsigned long long)rec[q].z << 32) | rec[q].w;
+            if (ka[q] == key)
+                a.far[rec[q].x] = rec[q].y;
+            if (kb[q] == key)
+                a.far[rec[q].y] = rec[q].x;
+        }
+    }
 }
 
 // Hook: each component that found an edge either stays root (lower id of a
@@ -480,40 +537,30 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
     const bool all = *(volatile uint32_t *)&ctl->cand_all;
     const uint64_t count = all ? a.n : ctl->roots[r];
     const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
-    const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
     unsigned long long active_cnt = 0;
     const uint64_t step = (uint64_t)gridDim.x * kBlock * kVItems;
     for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * kVItems; i0 < count; i0 += step) {
-        uint32_t x[kVItems];
-        unsigned long long bk[kVItems];
+        uint32_t x[kVItems], other[kVItems];
+        unsigned long long bk[kVItems], ob[kVItems];
 #pragma unroll
         for (int k = 0; k < kVItems; k++) {
             const uint64_t i = i0 + k * kBlock + threadIdx.x;
             x[k] = i < count ? (all ? (uint32_t)i : cand[i]) : 0;
             bk[k] = i < count ? a.best[x[k]] : kKeyNone;
         }
-        uint32_t pos[kVItems];
 #pragma unroll
         for (int k = 0; k < kVItems; k++)
-            pos[k] = bk[k] != kKeyNone ? a.pos_of_id[(uint32_t)bk[k]] : 0;
-        uint4 rec[kVItems];
+            other[k] = bk[k] != kKeyNone ? a.far[x[k]] : 0;
 #pragma unroll
         for (int k = 0; k < kVItems; k++)
-            rec[k] = bk[k] != kKeyNone ? wl[pos[k]] : make_uint4(0, 0, 0, 0);
-        uint32_t other[kVItems];
-        unsigned long long ob[kVItems];
-#pragma unroll
-        for (int k = 0; k < kVItems; k++) {
-            other[k] = rec[k].x == x[k] ? rec[k].y : rec[k].x;
             ob[k] = bk[k] != kKeyNone ? __ldcg(a.best + other[k]) : 0ull;
-        }
 #pragma unroll
         for (int k = 0; k < kVItems; k++) {
             if (bk[k] == kKeyNone)
                 continue;
             active_cnt++;
             const uint32_t id = (uint32_t)bk[k];
-            if (rec[k].x != x[k] && rec[k].y != x[k]) {
+            if (other[k] == x[k] || other[k] >= a.n) {
                 set_err(&ctl->err, kErrChase);
                 continue;
             }
@@ -717,7 +764,7 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.epoch_base = (uint32_t)p.epoch_base;
     a.parent = p.parent;
     a.best = p.best;
-    a.pos_of_id = p.pos_of_id;
+    a.far = p.far;
     a.cand0 = p.cand[0];
     a.cand1 = p.cand[1];
     a.bitmap = p.bitmap;
@@ -746,6 +793,10 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
             edge_pass_kernel<KIND, 4><<<ctx->edge_pass_blocks4, kBlock, pipe_smem<4>(), ctx->stream>>>(a);
         else
             edge_pass_kernel<KIND, 8><<<ctx->edge_pass_blocks, kBlock, pipe_smem<8>(), ctx->stream>>>(a);
+    }
+    {
+        KernelScope k(ctx, kKResolve);
+        resolve_kernel<<<ctx->sm_count * 4, kBlock, 0, ctx->stream>>>(a);
     }
     {
         KernelScope k(ctx, kKHook);
@@ -841,8 +892,8 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
 uint64_t wl_capacity(uint64_t m, int sm_count) { return m + (uint64_t)sm_count * kMaxEdgeCtasPerSm * kChunk; }
 
 // Workspace of one solve: parent (4n), best (8n), two candidate lists (4n
-// each), the MSF bitmap (m / 8), edge id -> survivor position (4m) and two
-// survivor lists (16 bytes per record each).  The carve order is fixed;
+// each), the MSF bitmap (m / 8), far roots (4n) and two survivor lists (16
+// bytes per record each).  The carve order is fixed;
 // msf_plan repeats it.
 size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
 {
@@ -852,7 +903,7 @@ size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
     c.take<uint32_t>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>((m + 31) / 32 + 4);
-    c.take<uint32_t>(m);
+    c.take<uint32_t>(n);
     c.take<uint4>(wl_capacity(m, sm_count));
     c.take<uint4>(wl_capacity(m, sm_count));
     return c.off;
@@ -875,7 +926,7 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     plan->cand[0] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
-    plan->pos_of_id = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(m));
+    plan->far = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->wl[1] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->e0 = d_e0;
