@@ -70,7 +70,7 @@ struct Timed {
 }  // namespace
 
 const char *const kKernelNames[kKernelCount] = {
-    "msf_init", "msf_select", "msf_edge_pass", "msf_resolve", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
+    "msf_init", "msf_select", "msf_edge_pass", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
     "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "csr_pack"};
 
 constexpr size_t kLaunchLogCap = 1u << 16;

@@ -14,7 +14,7 @@
 namespace phem {
 // Kernels the library launches; the profile reports them by these names.
 enum KernelId : int {
-    kKInit = 0, kKSelect, kKEdgePass, kKResolve, kKHook, kKCompress, kKAdvance, kKGather,
+    kKInit = 0, kKSelect, kKEdgePass, kKHook, kKCompress, kKAdvance, kKGather,
     kKCcInit, kKCcUnite, kKCcMerge, kKCcLabel, kKMinid, kKCcCount, kKCsrCoo, kKPack,
     kKernelCount
 };
@@ -135,7 +135,6 @@ struct MsfPlan {
     unsigned long long *best;// n
     uint32_t *cand[2];       // n each
     uint32_t *bitmap;        // ceil(m / 32)
-    uint32_t *far;           // n: far root of each component's chosen edge
     uint4 *wl[2];            // m each
     uint64_t *status;        // look-back status (context-owned), >= tiles
     uint64_t epoch_base;

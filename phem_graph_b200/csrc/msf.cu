@@ -28,15 +28,16 @@
 //      is in no MSF: the filter changes the work, not the result.
 //
 // A component's choice is the minimum key (w << 32 | id) offered to it, kept
-// with fire-and-forget 64-bit atomicMin.  A short record-parallel resolve pass
-// then stores, for each component, the far root of the survivor whose key won
-// there, so the hook needs no survivor record and the survivor list may be in
-// any order.  That removes every dependency between CTAs from the edge pass:
-// tiles are statically strided over a persistent grid, arrive in shared memory
-// by 1-D bulk copies (cp.async.bulk) two tiles ahead of use, survivors are
-// staged densely in shared memory before their coalesced write, and output
-// space is reserved in chunks with one atomicAdd each.  MSF membership is a bitmap over edge ids; one
-// ordered gather (decoupled look-back) writes the MSF records ascending by id
+// with fire-and-forget 64-bit atomicMin.  The hook then runs over the survivor
+// records: a record whose key won at an endpoint is that endpoint's choice, so
+// no record has to be looked up and the survivor list may be in any order.
+// That removes every dependency between CTAs from the edge pass: tiles are
+// statically strided over a persistent grid, arrive in shared memory by 1-D
+// bulk copies (cp.async.bulk) two tiles ahead of use, survivors are staged
+// densely in shared memory before their coalesced write, and output space is
+// reserved in chunks with one atomicAdd each.  MSF membership is a bitmap over
+// edge ids; one ordered gather (decoupled look-back) writes the MSF records
+// ascending by id
 // with the uint64 total.  Every round kernel reads the round, phase and
 // continue flag from the device control block, so rounds are queued ahead
 // without host round trips; a round queued after convergence exits at once.
@@ -55,7 +56,6 @@ struct RoundArgs {
     uint32_t epoch_base;
     uint32_t *parent;
     unsigned long long *best;  // per component: minimum key (w << 32 | id) offered this round
-    uint32_t *far;             // per component: far root of the edge it chose (set by resolve)
     uint32_t *cand0, *cand1;
     uint32_t *bitmap;
     uint4 *wl0, *wl1;
@@ -484,18 +484,25 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         out[s_base + i] = make_uint4(0, 0, 0, 0);
 }
 
-// Resolve: for every survivor of this round whose key won at an endpoint's
-// component, record the far component there.  Keys are unique, so exactly
-// one record writes each far[x].  Dead padding records (equal roots) are
-// skipped.  The list was just written, so it is mostly read from L2.
-__global__ void __launch_bounds__(kBlock) resolve_kernel(RoundArgs a)
+// Hook, over this round's survivor records: a record whose key is the
+// minimum at an endpoint's component is that component's chosen edge (keys
+// are unique, so each component finds exactly one).  A component hooks onto
+// the far one and marks the edge; when both endpoints chose the same record
+// (a mutual pair) the lower id stays root and the higher one hooks
+// (new_grafting_edges, MST/src/kernels.cu:73-134).  Dead padding records
+// (equal roots) are skipped.  The list was just written, so it is mostly read
+// from L2.
+template <int KIND>
+__global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
 {
+    __shared__ unsigned long long s_red[kWarps];
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const uint64_t len = ctl->wl_len[r];
     const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
+    unsigned long long chosen = 0;
     const uint64_t step = (uint64_t)gridDim.x * kBlock * 4;
     for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * 4; i0 < len; i0 += step) {
         uint4 rec[4];
@@ -513,69 +520,34 @@ __global__ void __launch_bounds__(kBlock) resolve_kernel(RoundArgs a)
             if (rec[q].x == rec[q].y)
                 continue;
             const unsigned long long key = ((unsigned long long)rec[q].z << 32) | rec[q].w;
-            if (ka[q] == key)
-                a.far[rec[q].x] = rec[q].y;
-            if (kb[q] == key)
-                a.far[rec[q].y] = rec[q].x;
-        }
-    }
-}
-
-// Hook: each component that found an edge either stays root (lower id of a
-// mutual pair) or points at the far component and marks its edge.  kVItems
-// candidates per thread per iteration keep several dependent chains in flight.
-constexpr int kVItems = 4;
-
-template <int KIND>
-__global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
-{
-    __shared__ unsigned long long s_red[kWarps];
-    Ctl *ctl = a.ctl;
-    if (!*(volatile uint32_t *)&ctl->go)
-        return;
-    const uint32_t r = *(volatile uint32_t *)&ctl->round;
-    const bool all = *(volatile uint32_t *)&ctl->cand_all;
-    const uint64_t count = all ? a.n : ctl->roots[r];
-    const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
-    unsigned long long active_cnt = 0;
-    const uint64_t step = (uint64_t)gridDim.x * kBlock * kVItems;
-    for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * kVItems; i0 < count; i0 += step) {
-        uint32_t x[kVItems], other[kVItems];
-        unsigned long long bk[kVItems], ob[kVItems];
-#pragma unroll
-        for (int k = 0; k < kVItems; k++) {
-            const uint64_t i = i0 + k * kBlock + threadIdx.x;
-            x[k] = i < count ? (all ? (uint32_t)i : cand[i]) : 0;
-            bk[k] = i < count ? a.best[x[k]] : kKeyNone;
-        }
-#pragma unroll
-        for (int k = 0; k < kVItems; k++)
-            other[k] = bk[k] != kKeyNone ? a.far[x[k]] : 0;
-#pragma unroll
-        for (int k = 0; k < kVItems; k++)
-            ob[k] = bk[k] != kKeyNone ? __ldcg(a.best + other[k]) : 0ull;
-#pragma unroll
-        for (int k = 0; k < kVItems; k++) {
-            if (bk[k] == kKeyNone)
+            const bool A = ka[q] == key, B = kb[q] == key;
+            if (!A && !B)
                 continue;
-            active_cnt++;
-            const uint32_t id = (uint32_t)bk[k];
-            if (other[k] == x[k] || other[k] >= a.n) {
-                set_err(&ctl->err, kErrChase);
-                continue;
+            chosen += (unsigned long long)A + (unsigned long long)B;
+            uint32_t hk, tgt;
+            if (A && B) {
+                hk = rec[q].x > rec[q].y ? rec[q].x : rec[q].y;
+                tgt = rec[q].x > rec[q].y ? rec[q].y : rec[q].x;
+            } else if (A) {
+                hk = rec[q].x;
+                tgt = rec[q].y;
+            } else {
+                hk = rec[q].y;
+                tgt = rec[q].x;
             }
-            if (ob[k] == bk[k] && x[k] < other[k])
-                continue;  // mutual pair: the lower id stays root, the partner hooks
-            a.parent[x[k]] = other[k];
+            const uint32_t id = rec[q].w;
+            a.parent[hk] = tgt;
             atomicOr(a.bitmap + (id >> 5), 1u << (id & 31));
             if (KIND == kKindPacked && a.forest)
-                a.forest[x[k]] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
+                a.forest[hk] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
         }
     }
-    const unsigned long long tot = block_sum_u64(active_cnt, s_red);
+    const unsigned long long tot = block_sum_u64(chosen, s_red);
     if (threadIdx.x == 0 && tot)
         atomicAdd(&ctl->n_r[r], tot);
 }
+
+constexpr int kVItems = 4;  // candidates per thread per iteration of the vertex kernels
 
 // Pointer jumping.  Normally over this round's components only: roots that
 // remain are collected as the next round's candidates (one atomicAdd per
@@ -764,7 +736,6 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.epoch_base = (uint32_t)p.epoch_base;
     a.parent = p.parent;
     a.best = p.best;
-    a.far = p.far;
     a.cand0 = p.cand[0];
     a.cand1 = p.cand[1];
     a.bitmap = p.bitmap;
@@ -795,12 +766,8 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
             edge_pass_kernel<KIND, 8><<<ctx->edge_pass_blocks, kBlock, pipe_smem<8>(), ctx->stream>>>(a);
     }
     {
-        KernelScope k(ctx, kKResolve);
-        resolve_kernel<<<ctx->sm_count * 4, kBlock, 0, ctx->stream>>>(a);
-    }
-    {
         KernelScope k(ctx, kKHook);
-        hook_kernel<KIND><<<vb, kBlock, 0, ctx->stream>>>(a);
+        hook_kernel<KIND><<<ctx->sm_count * 4, kBlock, 0, ctx->stream>>>(a);
     }
     {
         KernelScope k(ctx, kKCompress);
@@ -892,8 +859,8 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
 uint64_t wl_capacity(uint64_t m, int sm_count) { return m + (uint64_t)sm_count * kMaxEdgeCtasPerSm * kChunk; }
 
 // Workspace of one solve: parent (4n), best (8n), two candidate lists (4n
-// each), the MSF bitmap (m / 8), far roots (4n) and two survivor lists (16
-// bytes per record each).  The carve order is fixed;
+// each), the MSF bitmap (m / 8) and two survivor lists (16 bytes per record
+// each).  The carve order is fixed;
 // msf_plan repeats it.
 size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
 {
@@ -903,7 +870,6 @@ size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
     c.take<uint32_t>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>((m + 31) / 32 + 4);
-    c.take<uint32_t>(n);
     c.take<uint4>(wl_capacity(m, sm_count));
     c.take<uint4>(wl_capacity(m, sm_count));
     return c.off;
@@ -926,7 +892,6 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     plan->cand[0] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
-    plan->far = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->wl[1] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->e0 = d_e0;
