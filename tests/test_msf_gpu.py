@@ -70,7 +70,7 @@ def test_unfiltered_rounds_equal_boruvka_restatement(ctx, scale, ef):
     try:
         r = ctx.msf_solve(E, g.n)
     finally:
-        ctx.set_tuning("msf.light_per_vertex", 2.0)
+        ctx.set_tuning("msf.light_per_vertex", 1.0)
     assert r.m_r == [int(x) for x in m_r] + [0]
     assert r.n_r == [int(x) for x in n_r] + [0]
 
