@@ -207,6 +207,29 @@ phem_status phem_cc_merge(phem_context *ctx, const uint64_t *d_forest_a, const u
                           int32_t n, int32_t *d_parent, int32_t *d_label, uint64_t *d_forest_out,
                           float *ms);
 
+/* Largest n that phem_cc_solve_noalloc accepts: its scratch is a fixed
+ * file-scope device array of this many parent words (4 MiB). */
+#define PHEM_CC_NOALLOC_MAX_VERTICES (1 << 20)
+
+/* CC + spanning forest that allocates nothing.  No counterpart in the
+ * reference: it is phem_cc_solve's default path (same labels, a forest of the
+ * same kind) for callers that cannot allocate device memory at solve time --
+ * a serving process whose memory is committed under a budget, or a loop that
+ * cannot afford cudaMalloc/cudaFree stalling the device -- and so takes no
+ * context either.  The parent array lives in fixed static device scratch.
+ *   d_edges[m]  packed (u << 32 | v), DEVICE memory, 16-byte aligned;
+ *   d_labels[n] <- smallest vertex id of each component (DEVICE);
+ *   d_forest[n] <- forest slot per hooked root, PHEM_FOREST_EMPTY elsewhere
+ *                  (DEVICE, may be NULL);
+ *   stream      cudaStream_t the work is queued on (NULL: the default stream).
+ * Runs on the current device and returns when the work is complete.
+ * n > PHEM_CC_NOALLOC_MAX_VERTICES returns PHEM_ERR_INVALID.  The first call on
+ * a device looks the scratch address up (make it before any stream capture).
+ * All calls on a device share the scratch: calls that overlap in time race and
+ * corrupt each other's results. */
+phem_status phem_cc_solve_noalloc(const uint64_t *d_edges, int64_t m, int32_t n, int32_t *d_labels,
+                                  uint64_t *d_forest, void *stream);
+
 /* ------------------------------------------------------------ minimum spanning forest */
 
 /* Minimum spanning forest of edges[0..m) over vertices [0, n) under the strict

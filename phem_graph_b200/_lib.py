@@ -25,6 +25,7 @@ PHEM_FOREST_EMPTY = 0x7FFFFFFF
 PHEM_MAX_ROUNDS = 64
 PHEM_CC_DEFAULT = 0
 PHEM_CC_CANONICAL = 1
+PHEM_CC_NOALLOC_MAX_VERTICES = 1 << 20
 
 
 class PhemError(RuntimeError):
@@ -85,6 +86,7 @@ SIGNATURES = {
     "phem_cc_stream": (C.c_int, [_VP, _VP, C.c_int64, C.c_int32, C.c_int64, _VP, _VP, _VP,
                                  C.POINTER(C.c_float)]),
     "phem_cc_merge": (C.c_int, [_VP, _VP, _VP, C.c_int32, _VP, _VP, _VP, C.POINTER(C.c_float)]),
+    "phem_cc_solve_noalloc": (C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP, _VP]),
     "phem_msf_solve": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, _VP, C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64), C.POINTER(MSFStats)]),
     "phem_msf_solve_device": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, _VP, _VP, C.POINTER(MSFStats)]),
