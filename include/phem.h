@@ -116,6 +116,11 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
  *   "msf.next_batch"        rounds queued per later check                 [4]
  *   "msf.edge_items"        records per thread in the edge pass, 4 or 8   [8]
+ *   "batch.block_size"      threads per CTA of the batched kernel,
+ *                           256, 512 or 1024                               [512]
+ *   "batch.items"           records per thread per step, 1, 2 or 4         [2]
+ *   "batch.compact_ratio"   a batched list pass compacts when the live
+ *                           records are at most this share of the list     [0.5]
  * None of them changes a result. */
 phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double value);
 phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *value);
@@ -266,6 +271,89 @@ phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const 
 phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, int32_t n,
                             uint64_t *out, int64_t *out_m);
 
+/* ------------------------------------------------------------ batched small graphs */
+/* Many independent graphs solved in ONE persistent kernel launch: CTAs take
+ * whole graphs from a device work queue (largest first) and run Boruvka on
+ * each to completion.  No reference counterpart: the reference solves one
+ * graph per call (boruvka_for_edge_array, MST/src/new_boruvka.cu:40-179),
+ * and this is the batch of such calls without their launch overhead.  Every
+ * graph gets exactly what the one-graph entry points give it:
+ *   PHEM_BATCH_MSF  forest = the unique MSF under (w, edge index), as
+ *                   phem_msf_solve; total = its uint64 weight;
+ *   PHEM_BATCH_CC   forest = the canonical spanning forest (MSF under edge
+ *                   index order, phem_cc_solve with PHEM_CC_CANONICAL);
+ *                   total = 0;
+ * and labels = smallest vertex id of each vertex's component. */
+#define PHEM_BATCH_MSF 0u
+#define PHEM_BATCH_CC 1u
+
+/* One graph of a batch.  Its edges are edges[edge_offset, + num_edges) with
+ * vertex ids local to the graph (< num_vertices); an edge's id is its
+ * position within the graph.  Vertex-indexed outputs of the graph occupy
+ * [vertex_offset, + num_vertices); graphs' vertex ranges must not overlap. */
+typedef struct phem_batch_graph {
+    uint64_t edge_offset;
+    uint32_t num_edges;
+    uint32_t num_vertices;
+    uint32_t vertex_offset;
+    uint32_t kind;  /* PHEM_BATCH_MSF or PHEM_BATCH_CC */
+} phem_batch_graph;
+
+typedef struct phem_batch_stats {
+    uint32_t max_rounds;    /* most Boruvka rounds any graph needed */
+    uint32_t block_size;    /* kernel configuration used */
+    uint32_t items;
+    float compact_ratio;
+    uint32_t grid;          /* persistent CTAs launched */
+    uint32_t smem_vertices; /* graphs up to this many vertices kept their state in shared memory */
+    float device_ms;        /* GPU time of the batched launch (events on the stream) */
+} phem_batch_stats;
+
+/* Solves every graph of the batch.
+ *   graphs[num_graphs]       HOST array;
+ *   edges[total_edges]       host or device;
+ *   msf_ids[total_vertices]  <- graph g's forest edge ids, ascending, at
+ *                               [vertex_offset, + msf_count[g]) (may be NULL);
+ *   msf_count[num_graphs], msf_total[num_graphs] (required);
+ *   labels[total_vertices]   <- local min-id labels (may be NULL).
+ * Outputs may be host or device memory.  stats may be NULL. */
+phem_status phem_batch_solve(phem_context *ctx, const phem_batch_graph *graphs, uint32_t num_graphs,
+                             const phem_edge *edges, uint64_t total_edges, uint32_t total_vertices,
+                             uint32_t *msf_ids, uint32_t *msf_count, uint64_t *msf_total, int32_t *labels,
+                             phem_batch_stats *stats);
+
+/* Replayable batch plan: device buffers sized for a maximum batch plus a
+ * captured CUDA graph (queue reset + persistent kernel) that reads the batch
+ * size from device memory, so one capture serves every batch that fits.
+ * Kernel configuration comes from the context's batch.* tuning at creation;
+ * the context stream must not be the legacy default stream. */
+typedef struct phem_batch_plan phem_batch_plan;
+phem_status phem_batch_plan_create(phem_context *ctx, uint32_t max_graphs, uint64_t max_edges,
+                                   uint32_t max_vertices, phem_batch_plan **out);
+void phem_batch_plan_destroy(phem_batch_plan *plan);
+/* Queues the copies of a batch (host arrays; pinned edges overlap best) into
+ * the plan's buffers, asynchronously on the context stream. */
+phem_status phem_batch_plan_upload(phem_batch_plan *plan, const phem_batch_graph *graphs, uint32_t num_graphs,
+                                   const phem_edge *edges, uint64_t total_edges, uint32_t total_vertices);
+/* Replays the captured graph (asynchronous). */
+phem_status phem_batch_plan_run(phem_batch_plan *plan);
+/* Waits for the batch and copies results to host or device arrays (any may be
+ * NULL); returns the first error any graph reported. */
+phem_status phem_batch_plan_download(phem_batch_plan *plan, uint32_t *msf_ids, uint32_t *msf_count,
+                                     uint64_t *msf_total, int32_t *labels);
+/* Device addresses of the plan's buffers (for callers that keep inputs and
+ * results on the GPU).  Any pointer argument may be NULL. */
+phem_status phem_batch_plan_device(phem_batch_plan *plan, phem_edge **edges, uint32_t **msf_ids,
+                                   uint32_t **msf_count, uint64_t **msf_total, int32_t **labels);
+
+/* Autotuner: times every kernel configuration (block 256/512/1024 x items
+ * 1/2/4 x compaction ratio 0.25/0.5/1.0) on this batch, `reps` launches each,
+ * stores the fastest in the context's batch.* tuning and reports it in
+ * *best (whose device_ms is the best mean time).  Results are not returned. */
+phem_status phem_batch_autotune(phem_context *ctx, const phem_batch_graph *graphs, uint32_t num_graphs,
+                                const phem_edge *edges, uint64_t total_edges, uint32_t total_vertices,
+                                uint32_t reps, phem_batch_stats *best);
+
 /* --------------------------------------------------------- synthetic inputs (host) */
 /* Seeded generators for tests and benchmarks (no reference counterpart: the
  * reference reads graph files).  Deterministic for any thread count. */
@@ -295,6 +383,12 @@ phem_status phem_pack_msf_edges(const uint64_t *pairs, const uint32_t *w, uint64
 /* Symmetrised CSR from pairs sorted by (u, v) with u < v. */
 phem_status phem_csr_from_sorted_pairs(const uint64_t *pairs, uint64_t m, uint32_t n, int64_t *offsets,
                                        uint32_t *cols);
+
+/* 2-D random geometric graph: n points uniform in the unit square, each
+ * linked to its k nearest neighbours (ties by lower index), every pair once,
+ * sorted and packed (min << 32 | max); w[e] = floor(distance * 2^24) computed
+ * in double precision.  out and w need n * k entries (either may be NULL). */
+phem_status phem_gen_rgg(uint32_t n, uint32_t k, uint64_t seed, uint64_t *out, uint32_t *w, uint64_t *out_m);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,8 @@ PHEM_MAX_ROUNDS = 64
 PHEM_CC_DEFAULT = 0
 PHEM_CC_CANONICAL = 1
 PHEM_CC_NOALLOC_MAX_VERTICES = 1 << 20
+PHEM_BATCH_MSF = 0
+PHEM_BATCH_CC = 1
 
 
 class PhemError(RuntimeError):
@@ -57,6 +59,17 @@ class KernelProfile(C.Structure):
 
 class LaunchRecord(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("ms", C.c_float)]
+
+
+class BatchGraph(C.Structure):
+    _fields_ = [("edge_offset", C.c_uint64), ("num_edges", C.c_uint32), ("num_vertices", C.c_uint32),
+                ("vertex_offset", C.c_uint32), ("kind", C.c_uint32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("max_rounds", C.c_uint32), ("block_size", C.c_uint32), ("items", C.c_uint32),
+                ("compact_ratio", C.c_float), ("grid", C.c_uint32), ("smem_vertices", C.c_uint32),
+                ("device_ms", C.c_float)]
 
 
 _VP = C.c_void_p
@@ -100,6 +113,18 @@ SIGNATURES = {
     "phem_gen_weights": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, _VP]),
     "phem_pack_msf_edges": (C.c_int, [_VP, _VP, C.c_uint64, _VP]),
     "phem_csr_from_sorted_pairs": (C.c_int, [_VP, C.c_uint64, C.c_uint32, _VP, _VP]),
+    "phem_gen_rgg": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, _VP, _VP, C.POINTER(C.c_uint64)]),
+    "phem_batch_solve": (C.c_int, [_VP, _VP, C.c_uint32, _VP, C.c_uint64, C.c_uint32, _VP, _VP, _VP, _VP,
+                                   C.POINTER(BatchStats)]),
+    "phem_batch_plan_create": (C.c_int, [_VP, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(_VP)]),
+    "phem_batch_plan_destroy": (None, [_VP]),
+    "phem_batch_plan_upload": (C.c_int, [_VP, _VP, C.c_uint32, _VP, C.c_uint64, C.c_uint32]),
+    "phem_batch_plan_run": (C.c_int, [_VP]),
+    "phem_batch_plan_download": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "phem_batch_plan_device": (C.c_int, [_VP, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
+                                         C.POINTER(_VP)]),
+    "phem_batch_autotune": (C.c_int, [_VP, _VP, C.c_uint32, _VP, C.c_uint64, C.c_uint32, C.c_uint32,
+                                      C.POINTER(BatchStats)]),
 }
 
 

@@ -11,7 +11,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import (CCStats, KernelProfile, MSFStats, PHEM_CC_CANONICAL, PHEM_FOREST_EMPTY, check, lib, ptr)
+from ._lib import (BatchStats, CCStats, KernelProfile, MSFStats, PHEM_CC_CANONICAL, PHEM_FOREST_EMPTY, check, lib,
+                   ptr)
 
 # phem_edge as a numpy structured dtype (MST/src/constants.h:15-19)
 EDGE_DTYPE = np.dtype([("u", "<u4"), ("v", "<u4"), ("w", "<u4")])
@@ -48,6 +49,90 @@ class MSFResult:
     device_ms: float = 0.0
     light_rounds: int = 0
     threshold: int = 0
+
+
+@dataclass
+class BatchResult:
+    ids: np.ndarray            # vertex-indexed: graph g's forest ids at [vertex_offset, + count[g])
+    count: np.ndarray          # (G,) uint32
+    total: np.ndarray          # (G,) uint64
+    labels: np.ndarray | None  # vertex-indexed local min-id labels
+    stats: dict
+
+    def forest(self, batch, g: int) -> np.ndarray:
+        """Forest edge ids of graph g, ascending."""
+        o = int(batch.graphs[g]["vertex_offset"])
+        return self.ids[o: o + int(self.count[g])]
+
+    def graph_labels(self, batch, g: int) -> np.ndarray:
+        r = batch.graphs[g]
+        o = int(r["vertex_offset"])
+        return self.labels[o: o + int(r["num_vertices"])]
+
+
+def _stats_dict(st: BatchStats) -> dict:
+    return {"max_rounds": int(st.max_rounds), "block_size": int(st.block_size), "items": int(st.items),
+            "compact_ratio": float(st.compact_ratio), "grid": int(st.grid), "smem_vertices": int(st.smem_vertices),
+            "device_ms": float(st.device_ms)}
+
+
+def _batch_args(batch):
+    graphs = np.ascontiguousarray(batch.graphs)
+    edges = batch.edges if hasattr(batch.edges, "data_ptr") else np.ascontiguousarray(batch.edges, np.uint32)
+    return graphs, edges
+
+
+class BatchPlan:
+    """A replayable batch (phem_batch_plan): device buffers for up to
+    max_graphs / max_edges / max_vertices and one captured CUDA graph."""
+
+    def __init__(self, ctx: "Context", max_graphs: int, max_edges: int, max_vertices: int):
+        self._h = C.c_void_p()
+        check(lib().phem_batch_plan_create(ctx.handle, max_graphs, max_edges, max_vertices, C.byref(self._h)),
+              "phem_batch_plan_create")
+        self._batch = None
+
+    def upload(self, batch) -> None:
+        self._graphs, self._edges = _batch_args(batch)  # kept alive until the copies are done
+        check(lib().phem_batch_plan_upload(self._h, ptr(self._graphs), len(self._graphs), ptr(self._edges),
+                                           len(self._edges), batch.total_vertices), "phem_batch_plan_upload")
+        self._batch = batch
+
+    def run(self) -> None:
+        check(lib().phem_batch_plan_run(self._h), "phem_batch_plan_run")
+
+    def download(self, labels: bool = True) -> BatchResult:
+        b = self._batch
+        G, V = b.num_graphs, b.total_vertices
+        ids = np.empty(max(V, 1), np.uint32)
+        cnt = np.empty(max(G, 1), np.uint32)
+        tot = np.empty(max(G, 1), np.uint64)
+        lab = np.empty(max(V, 1), np.int32) if labels else None
+        check(lib().phem_batch_plan_download(self._h, ptr(ids), ptr(cnt), ptr(tot), ptr(lab)),
+              "phem_batch_plan_download")
+        return BatchResult(ids[:V], cnt[:G], tot[:G], lab[:V] if labels else None, {})
+
+    def device(self) -> dict:
+        ps = [C.c_void_p() for _ in range(5)]
+        check(lib().phem_batch_plan_device(self._h, *[C.byref(p) for p in ps]), "phem_batch_plan_device")
+        return dict(zip(["edges", "msf_ids", "msf_count", "msf_total", "labels"], [p.value for p in ps]))
+
+    def close(self) -> None:
+        if self._h:
+            lib().phem_batch_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:
@@ -209,6 +294,33 @@ class Context:
         k = C.c_int64()
         check(lib().phem_csr_to_coo(self._h, ptr(offsets), ptr(cols), n, ptr(out), C.byref(k)), "phem_csr_to_coo")
         return out[: k.value]
+
+    # ------------------------------------------------------------ batches
+
+    def batch_solve(self, batch, labels: bool = True) -> BatchResult:
+        """Every graph of a gen.Batch in one persistent launch."""
+        graphs, edges = _batch_args(batch)
+        G, V = len(graphs), batch.total_vertices
+        ids = np.empty(max(V, 1), np.uint32)
+        cnt = np.empty(max(G, 1), np.uint32)
+        tot = np.empty(max(G, 1), np.uint64)
+        lab = np.empty(max(V, 1), np.int32) if labels else None
+        st = BatchStats()
+        check(lib().phem_batch_solve(self._h, ptr(graphs), G, ptr(edges), len(edges), V, ptr(ids), ptr(cnt),
+                                     ptr(tot), ptr(lab), C.byref(st)), "phem_batch_solve")
+        return BatchResult(ids[:V], cnt[:G], tot[:G], lab[:V] if labels else None, _stats_dict(st))
+
+    def batch_autotune(self, batch, reps: int = 3) -> dict:
+        """Times every batched-kernel configuration on `batch`, keeps the
+        fastest in this context's batch.* tuning and returns it."""
+        graphs, edges = _batch_args(batch)
+        st = BatchStats()
+        check(lib().phem_batch_autotune(self._h, ptr(graphs), len(graphs), ptr(edges), len(edges),
+                                        batch.total_vertices, reps, C.byref(st)), "phem_batch_autotune")
+        return _stats_dict(st)
+
+    def batch_plan(self, max_graphs: int, max_edges: int, max_vertices: int) -> BatchPlan:
+        return BatchPlan(self, max_graphs, max_edges, max_vertices)
 
 
 def _msf_result(edges, count: int, total: int, st) -> MSFResult:

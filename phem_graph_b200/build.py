@@ -30,9 +30,9 @@ NVCC_FLAGS = ARCH + [
 ]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-I", str(ROOT / "include")]
 
-CU_SOURCES = ["api.cu", "cc.cu", "msf.cu", "csr.cu", "noalloc.cu"]
+CU_SOURCES = ["api.cu", "cc.cu", "msf.cu", "csr.cu", "noalloc.cu", "batch.cu", "batch_api.cu"]
 CXX_SOURCES = ["gen.cpp"]
-HEADERS = ["common.cuh", "internal.h"]
+HEADERS = ["common.cuh", "internal.h", "batch.h"]
 
 
 def nvcc() -> str:

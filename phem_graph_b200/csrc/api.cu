@@ -18,60 +18,12 @@ namespace phem {
 namespace {
 thread_local char g_last_error[512] = "";
 
-// Makes ctx->device current for the duration of a call, restoring the caller's.
-struct DeviceGuard {
-    int prev = -1;
-    bool ok = true;
-    explicit DeviceGuard(int dev)
-    {
-        if (cudaGetDevice(&prev) != cudaSuccess)
-            prev = -1;
-        if (prev != dev)
-            ok = cudaSetDevice(dev) == cudaSuccess;
-    }
-    ~DeviceGuard()
-    {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev)
-            cudaSetDevice(prev);
-    }
-};
-
-// A caller array staged through the workspace when it is host memory.
-struct Staged {
-    void *dev = nullptr;   // pointer the kernels use
-    void *host = nullptr;  // caller's host pointer (null when it was already device memory)
-    size_t bytes = 0;
-};
-
-phem_status check_ctx(phem_context *ctx)
-{
-    if (!ctx) {
-        set_error("null context");
-        return PHEM_ERR_INVALID;
-    }
-    return PHEM_OK;
-}
-
-// Event-timed region on the context stream.
-struct Timed {
-    phem_context *ctx;
-    explicit Timed(phem_context *c) : ctx(c) { cudaEventRecord(ctx->ev_start, ctx->stream); }
-    float stop()
-    {
-        float ms = 0.f;
-        cudaEventRecord(ctx->ev_stop, ctx->stream);
-        if (cudaEventSynchronize(ctx->ev_stop) == cudaSuccess)
-            cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
-        return ms;
-    }
-};
-
 }  // namespace
 
 const char *const kKernelNames[kKernelCount] = {
     "msf_init", "msf_select", "msf_edge_pass", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
-    "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "csr_pack"};
+    "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "csr_pack",
+    "batch_solve"};
 
 constexpr size_t kLaunchLogCap = 1u << 16;
 
@@ -249,45 +201,6 @@ phem_status ctl_status(uint32_t err, const char *what)
 }
 
 namespace {
-
-// Stages `bytes` of a caller input into the workspace at `off` when it is host
-// memory (queued on the context stream).
-phem_status stage_in(phem_context *ctx, const void *p, size_t bytes, size_t off, Staged *st)
-{
-    st->bytes = bytes;
-    if (is_device_ptr(p)) {
-        st->dev = const_cast<void *>(p);
-        st->host = nullptr;
-        return PHEM_OK;
-    }
-    st->dev = static_cast<char *>(ctx->ws) + off;
-    st->host = nullptr;
-    if (bytes)
-        PHEM_CUDA_TRY(cudaMemcpyAsync(st->dev, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    return PHEM_OK;
-}
-
-// An output: device pointer used directly, host pointer via workspace at `off`.
-void stage_out(phem_context *ctx, void *p, size_t bytes, size_t off, Staged *st)
-{
-    st->bytes = bytes;
-    if (!p || is_device_ptr(p)) {
-        st->dev = p;
-        st->host = nullptr;
-        return;
-    }
-    st->dev = static_cast<char *>(ctx->ws) + off;
-    st->host = p;
-}
-
-phem_status copy_back(phem_context *ctx, const Staged &st, size_t bytes)
-{
-    if (st.host && bytes)
-        PHEM_CUDA_TRY(cudaMemcpyAsync(st.host, st.dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    return PHEM_OK;
-}
-
-size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Edge ids and survivor-list positions are 32-bit; a survivor list holds the
 // edges plus up to 2^24 records of padding.
@@ -493,6 +406,12 @@ phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double v
         ctx->tune_next_batch = (int)value;
     } else if (k == "msf.edge_items" && (value == 4 || value == 8)) {
         ctx->tune_edge_items = (int)value;
+    } else if (k == "batch.block_size" && (value == 256 || value == 512 || value == 1024)) {
+        ctx->tune_batch_block = (int)value;
+    } else if (k == "batch.items" && (value == 1 || value == 2 || value == 4)) {
+        ctx->tune_batch_items = (int)value;
+    } else if (k == "batch.compact_ratio" && value >= 0.0 && value <= 1.0) {
+        ctx->tune_batch_compact = value;
     } else {
         set_error("set_tuning: unknown key or value out of range: %s = %g", key, value);
         return PHEM_ERR_INVALID;
@@ -518,6 +437,12 @@ phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *
         *value = ctx->tune_next_batch;
     else if (k == "msf.edge_items")
         *value = ctx->tune_edge_items;
+    else if (k == "batch.block_size")
+        *value = ctx->tune_batch_block;
+    else if (k == "batch.items")
+        *value = ctx->tune_batch_items;
+    else if (k == "batch.compact_ratio")
+        *value = ctx->tune_batch_compact;
     else {
         set_error("get_tuning: unknown key %s", key);
         return PHEM_ERR_INVALID;

@@ -1,0 +1,373 @@
+// batch.cu -- thousands of small graphs (MSF or CC each) in one persistent launch.
+//
+// The reference solves one graph per call (boruvka_for_edge_array,
+// MST/src/new_boruvka.cu:40-179; SpanningTree, CC/ExternalSpanningTree.cu:133-218),
+// paying ~10 launches and several host synchronisations per Boruvka round.
+// Small graphs are then pure launch overhead.  Here every CTA of one
+// persistent grid takes whole graphs from a device work queue (largest
+// first) and solves each to completion on its own, with __syncthreads as the
+// only barrier:
+//
+//   round 0   stream the graph's 12-byte input records once; self-loops are
+//             dropped, every other edge offers its key to both endpoints
+//             (atomicMin on per-vertex best keys) and is written, compacted,
+//             to a 16-byte survivor list {root_u, root_v, w, id};
+//   hook      every component with an offer takes its minimum edge; a mutual
+//             pair keeps the lower root (new_grafting_edges,
+//             MST/src/kernels.cu:73-134); the edge is marked in a bitmap;
+//   compress  every vertex is jumped to its root (new_shortcutting_step,
+//             MST/src/kernels.cu:254-271) and best is reset;
+//   relabel   the survivor list is relabelled to roots; internal edges die
+//             (relabelling_step/filtering_step, MST/src/kernels.cu:273-321);
+//             the list is compacted in place when enough records died.
+//
+// Keys are (w << 32 | id) for MSF graphs and id alone for CC graphs, so a CC
+// graph's forest is the canonical one (the MSF under edge index order) and
+// its labels are the minimum vertex id of each component.  The per-vertex
+// state (parent, root, best key: 16 bytes a vertex) lives in dynamic shared
+// memory when the graph fits, else in a global region of the graph's own.
+//
+// Tuning: block size B and records per thread I are template parameters, the
+// compaction threshold is a run-time ratio; the autotuner in batch_api.cu
+// picks all three.
+#include "batch.h"
+
+namespace phem {
+namespace {
+
+constexpr unsigned long long kKeyInf = ~0ull;
+constexpr uint32_t kBatchMaxRounds = 64;
+constexpr uint32_t kNoVertex = 0xffffffffu;
+
+template <int B>
+struct ScanSmem {
+    uint32_t part[2][B / 32 + 1];  // double-buffered warp partials
+};
+
+// Exclusive block scan of x; *total gets the block sum.  `parity` selects
+// the scratch half so two scans in a row need only the barriers inside.
+template <int B>
+__device__ __forceinline__ uint32_t block_scan(uint32_t x, ScanSmem<B> &s, int parity, uint32_t *total)
+{
+    constexpr int NW = B / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d)
+            inc += y;
+    }
+    if (lane == 31)
+        s.part[parity][warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t v = lane < NW ? s.part[parity][lane] : 0;
+        uint32_t vi = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, vi, d);
+            if (lane >= d)
+                vi += y;
+        }
+        if (lane < NW)
+            s.part[parity][lane] = vi - v;
+        if (lane == NW - 1)
+            s.part[parity][NW] = vi;
+    }
+    __syncthreads();
+    *total = s.part[parity][NW];
+    return s.part[parity][warp] + inc - x;
+}
+
+__device__ __forceinline__ unsigned long long graph_key(uint32_t kind, uint32_t w, uint32_t id)
+{
+    return kind == PHEM_BATCH_CC ? (unsigned long long)id : (((unsigned long long)w << 32) | id);
+}
+
+__device__ __forceinline__ void offer(unsigned long long *best, uint32_t t, unsigned long long key)
+{
+    if (key < *(volatile unsigned long long *)(best + t))
+        atomicMin(best + t, key);
+}
+
+template <int B>
+struct BatchSmem {
+    ScanSmem<B> scan;
+    unsigned long long red[B / 32];
+    uint32_t item;
+    uint32_t err;
+};
+
+// One relabel/filter pass over the graph's edges.  FIRST reads the input
+// records (ids = positions) and always compacts into the survivor list;
+// later passes read the list and compact in place when `compact` is set
+// (writes never overtake reads: an iteration's survivors land below the end
+// of its own slots, and all its reads precede the scan barrier).  Returns the
+// survivor count; *len_out gets the new list length.
+template <int B, int I, bool FIRST>
+__device__ uint32_t relabel_pass(const phem_edge *e0, uint4 *wl, uint32_t len, bool compact, uint32_t n,
+                                 uint32_t kind, const uint32_t *comp, unsigned long long *best,
+                                 BatchSmem<B> &sm, uint32_t *len_out)
+{
+    uint32_t out = 0, live = 0;
+    int parity = 0;
+    for (uint32_t base = 0; base < len; base += B * I) {
+        uint4 rec[I];
+        bool keep[I];
+#pragma unroll
+        for (int j = 0; j < I; j++) {
+            const uint32_t i = base + j * B + threadIdx.x;
+            keep[j] = false;
+            rec[j] = make_uint4(0, 0, 0, 0);
+            if (i < len) {
+                if (FIRST) {
+                    const uint32_t u = __ldg(&e0[i].u), v = __ldg(&e0[i].v), w = __ldg(&e0[i].w);
+                    if (u >= n || v >= n) {
+                        atomicOr(&sm.err, kErrRange);
+                    } else if (u != v) {
+                        rec[j] = make_uint4(u, v, w, i);
+                        keep[j] = true;
+                    }
+                } else {
+                    rec[j] = wl[i];
+                    rec[j].x = comp[rec[j].x];
+                    rec[j].y = comp[rec[j].y];
+                    keep[j] = rec[j].x != rec[j].y;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < I; j++)
+            if (keep[j]) {
+                const unsigned long long key = graph_key(kind, rec[j].z, rec[j].w);
+                offer(best, rec[j].x, key);
+                offer(best, rec[j].y, key);
+            }
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int j = 0; j < I; j++)
+            cnt += keep[j];
+        uint32_t total = 0;
+        uint32_t pos = block_scan<B>(cnt, sm.scan, parity, &total);
+        parity ^= 1;
+        if (FIRST || compact) {
+#pragma unroll
+            for (int j = 0; j < I; j++)
+                if (keep[j])
+                    wl[out + pos++] = rec[j];
+            out += total;
+        }
+        live += total;
+    }
+    *len_out = (FIRST || compact) ? out : len;
+    return live;
+}
+
+template <int B, int I>
+__device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B> &sm, unsigned char *dyn)
+{
+    const uint32_t n = it.n, m = it.m;
+    const phem_edge *e0 = a.edges + it.e_off;
+    uint4 *wl = a.wl + it.wl_off;
+    uint32_t *bm = a.bitmap + it.bm_off;
+    const bool local = n <= a.smem_vertices;
+    uint32_t *parent = local ? reinterpret_cast<uint32_t *>(dyn) : a.g_parent + it.v_off;
+    uint32_t *comp = local ? reinterpret_cast<uint32_t *>(dyn) + a.smem_vertices : a.g_comp + it.v_off;
+    unsigned long long *best = local ? reinterpret_cast<unsigned long long *>(dyn + 8 * (size_t)a.smem_vertices)
+                                     : a.g_best + it.v_off;
+    const uint32_t nwords = (m + 31) / 32;
+
+    for (uint32_t x = threadIdx.x; x < n; x += B) {
+        parent[x] = x;
+        comp[x] = x;
+        best[x] = kKeyInf;
+    }
+    for (uint32_t w = threadIdx.x; w < nwords; w += B)
+        bm[w] = 0;
+    __syncthreads();
+
+    uint32_t len = 0;
+    uint32_t live = relabel_pass<B, I, true>(e0, wl, m, true, n, it.kind, comp, best, sm, &len);
+    uint32_t rounds = 0;
+    while (live > 0) {
+        if (++rounds > kBatchMaxRounds) {
+            if (threadIdx.x == 0)
+                atomicOr(&sm.err, kErrRounds);
+            break;
+        }
+        __syncthreads();  // offers complete
+        // hook: each component with an offer takes its minimum edge
+        for (uint32_t x = threadIdx.x; x < n; x += B) {
+            const unsigned long long k = best[x];
+            if (k == kKeyInf)
+                continue;
+            const uint32_t id = (uint32_t)k;
+            const uint32_t cu = comp[__ldg(&e0[id].u)], cv = comp[__ldg(&e0[id].v)];
+            const uint32_t other = cu == x ? cv : cu;
+            if (best[other] == k && x < other)
+                continue;  // mutual pair: the lower root stays a root
+            parent[x] = other;
+            atomicOr(bm + (id >> 5), 1u << (id & 31));
+        }
+        __syncthreads();
+        // compress: every vertex to its root, best reset
+        for (uint32_t x = threadIdx.x; x < n; x += B) {
+            uint32_t r = x;
+            for (uint32_t steps = 0; steps <= n; steps++) {
+                const uint32_t p = *(volatile uint32_t *)(parent + r);
+                if (p == r)
+                    break;
+                r = p;
+            }
+            if (*(volatile uint32_t *)(parent + r) != r)
+                atomicOr(&sm.err, kErrChase);
+            comp[x] = r;
+            if (parent[x] != r)
+                parent[x] = r;
+            best[x] = kKeyInf;
+        }
+        __syncthreads();
+        const bool compact = (float)live <= a.compact_ratio * (float)len;
+        live = relabel_pass<B, I, false>(e0, wl, len, compact, n, it.kind, comp, best, sm, &len);
+    }
+    __syncthreads();
+
+    // labels: minimum vertex id of each component (comp is final)
+    for (uint32_t x = threadIdx.x; x < n; x += B)
+        parent[x] = kNoVertex;
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < n; x += B)
+        atomicMin(parent + comp[x], x);
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < n; x += B)
+        a.labels[it.v_off + x] = (int32_t)parent[comp[x]];
+
+    // forest edges ascending by id, and the total weight
+    uint32_t out = 0;
+    unsigned long long wsum = 0;
+    int parity = 0;
+    for (uint32_t w0 = 0; w0 < nwords; w0 += B) {
+        const uint32_t wi = w0 + threadIdx.x;
+        uint32_t word = wi < nwords ? bm[wi] : 0u;
+        uint32_t total = 0;
+        uint32_t pos = block_scan<B>((uint32_t)__popc(word), sm.scan, parity, &total);
+        parity ^= 1;
+        while (word) {
+            const uint32_t b = __ffs(word) - 1;
+            word &= word - 1;
+            const uint32_t id = wi * 32 + b;
+            if (out + pos < n)  // a forest has at most n - 1 edges
+                a.msf_ids[it.v_off + out + pos] = id;
+            else
+                atomicOr(&sm.err, kErrCapacity);
+            pos++;
+            if (it.kind != PHEM_BATCH_CC)
+                wsum += __ldg(&e0[id].w);
+        }
+        out += total;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+        wsum += __shfl_xor_sync(0xffffffffu, wsum, d);
+    if ((threadIdx.x & 31) == 0)
+        sm.red[threadIdx.x >> 5] = wsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < B / 32; i++)
+            t += sm.red[i];
+        a.msf_count[it.index] = out;
+        a.msf_total[it.index] = t;
+        a.status[it.index] = sm.err;
+        if (a.rounds)
+            a.rounds[it.index] = rounds;
+    }
+}
+
+template <int B, int I>
+__global__ void __launch_bounds__(B) batch_kernel(BatchArgs a)
+{
+    __shared__ BatchSmem<B> sm;
+    extern __shared__ __align__(16) unsigned char dyn[];
+    const uint32_t G = *a.num_graphs;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            sm.item = atomicAdd(a.queue, 1u);
+            sm.err = 0;
+        }
+        __syncthreads();
+        const uint32_t q = sm.item;
+        if (q >= G)
+            break;
+        const BatchItem it = a.items[q];
+        solve_graph<B, I>(a, it, sm, dyn);
+        __syncthreads();  // sm.item, sm.err and the shared state are free again
+    }
+}
+
+template <int B, int I>
+const void *kernel_ptr()
+{
+    return reinterpret_cast<const void *>(&batch_kernel<B, I>);
+}
+
+const void *select_kernel(int block, int items)
+{
+#define PHEM_BATCH_CASE(b, i)         \
+    if (block == b && items == i)     \
+        return kernel_ptr<b, i>();
+    PHEM_BATCH_CASE(256, 1) PHEM_BATCH_CASE(256, 2) PHEM_BATCH_CASE(256, 4)
+    PHEM_BATCH_CASE(512, 1) PHEM_BATCH_CASE(512, 2) PHEM_BATCH_CASE(512, 4)
+    PHEM_BATCH_CASE(1024, 1) PHEM_BATCH_CASE(1024, 2) PHEM_BATCH_CASE(1024, 4)
+#undef PHEM_BATCH_CASE
+    return nullptr;
+}
+
+}  // namespace
+
+phem_status batch_launch_config(int device, int sm_count, int block, int items, BatchLaunch *out)
+{
+    const void *k = select_kernel(block, items);
+    if (!k) {
+        set_error("batch: no kernel for block %d, items %d (blocks 256/512/1024, items 1/2/4)", block, items);
+        return PHEM_ERR_INVALID;
+    }
+    int per_sm_smem = 0, optin = 0;
+    PHEM_CUDA_TRY(cudaDeviceGetAttribute(&per_sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+    PHEM_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa;
+    PHEM_CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+    // aim for the thread-limited number of CTAs per SM; each gets an equal
+    // share of shared memory for its vertex state (16 bytes a vertex)
+    const int want = 2048 / block;
+    size_t dyn = (size_t)per_sm_smem / want;
+    dyn = dyn > 1024 + fa.sharedSizeBytes ? dyn - 1024 - fa.sharedSizeBytes : 0;
+    if (dyn > (size_t)optin - fa.sharedSizeBytes)
+        dyn = (size_t)optin - fa.sharedSizeBytes;
+    dyn &= ~size_t(15);
+    PHEM_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    int occ = 0;
+    PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, dyn));
+    if (occ < 1) {
+        set_error("batch: kernel (block %d, items %d) does not fit on an SM", block, items);
+        return PHEM_ERR_UNSUPPORTED;
+    }
+    out->kernel = k;
+    out->block = block;
+    out->items = items;
+    out->dyn_smem = dyn;
+    out->smem_vertices = (uint32_t)(dyn / 16);
+    out->grid = sm_count * occ;
+    return PHEM_OK;
+}
+
+phem_status batch_launch(cudaStream_t stream, const BatchLaunch &l, BatchArgs args)
+{
+    args.smem_vertices = l.smem_vertices;
+    void *params[] = {&args};
+    PHEM_CUDA_TRY(cudaLaunchKernel(l.kernel, dim3(l.grid), dim3(l.block), params, l.dyn_smem, stream));
+    return PHEM_OK;
+}
+
+}  // namespace phem

@@ -45,6 +45,7 @@ inline uint32_t lemire(uint32_t x, uint32_t range) { return (uint32_t)(((uint64_
 constexpr uint64_t kTagER = 0x45522D45444745ull;    // "ER-EDGE"
 constexpr uint64_t kTagRMAT = 0x524D41542D4544ull;  // "RMAT-ED"
 constexpr uint64_t kTagW = 0x5745494748542Dull;     // "WEIGHT-"
+constexpr uint64_t kTagRGG = 0x5247472D505453ull;   // "RGG-PTS"
 
 int num_threads()
 {
@@ -268,6 +269,92 @@ phem_status phem_csr_from_sorted_pairs(const uint64_t *pairs, uint64_t m, uint32
         cols[lowpos[v]++] = u;
         cols[highpos[u]++] = v;
     }
+    return PHEM_OK;
+}
+
+// 2-D random geometric k-nearest-neighbour graph.  Point i is
+// (x, y) = (value 2i, value 2i + 1) of the stream, each scaled from its top 53
+// bits to [0, 1).  Every point links to its k nearest other points (distance
+// ties broken by the lower index); a pair chosen from both sides is emitted
+// once.  Weights are floor(distance * 2^24) in double precision on the host
+// (IEEE sqrt is correctly rounded, so the weights are the same everywhere).
+// Pairs come out packed (min << 32 | max), sorted; out and w need n * k
+// entries (NULL to count).
+phem_status phem_gen_rgg(uint32_t n, uint32_t k, uint64_t seed, uint64_t *out, uint32_t *w, uint64_t *out_m)
+{
+    if (n < 2 || k < 1 || k >= n || !out_m)
+        return PHEM_ERR_INVALID;
+    const uint64_t base = stream_base(seed, kTagRGG);
+    std::vector<double> px(n), py(n);
+    for (uint32_t i = 0; i < n; i++) {
+        px[i] = (double)(stream_at(base, 2ull * i) >> 11) * 0x1.0p-53;
+        py[i] = (double)(stream_at(base, 2ull * i + 1) >> 11) * 0x1.0p-53;
+    }
+    // uniform grid with about four points per cell: the 3 x 3 block around a
+    // point usually holds its 8 nearest neighbours
+    const uint32_t side = std::max(1u, (uint32_t)std::sqrt((double)n / 4.0));
+    std::vector<uint32_t> cell_start((size_t)side * side + 1, 0), cell_pts(n);
+    auto cell_of = [&](uint32_t i) {
+        const uint32_t cx = std::min(side - 1, (uint32_t)(px[i] * side));
+        const uint32_t cy = std::min(side - 1, (uint32_t)(py[i] * side));
+        return cy * side + cx;
+    };
+    for (uint32_t i = 0; i < n; i++)
+        cell_start[cell_of(i) + 1]++;
+    for (uint32_t c = 0; c < side * side; c++)
+        cell_start[c + 1] += cell_start[c];
+    {
+        std::vector<uint32_t> fill(cell_start.begin(), cell_start.end() - 1);
+        for (uint32_t i = 0; i < n; i++)
+            cell_pts[fill[cell_of(i)]++] = i;
+    }
+    std::vector<uint64_t> pairs((uint64_t)n * k);
+    parallel_ranges(n, [&](int, uint64_t lo, uint64_t hi) {
+        std::vector<std::pair<double, uint32_t>> cand;
+        for (uint64_t i = lo; i < hi; i++) {
+            const int cx = (int)std::min(side - 1, (uint32_t)(px[i] * side));
+            const int cy = (int)std::min(side - 1, (uint32_t)(py[i] * side));
+            // grow the searched square ring by ring until k candidates are
+            // strictly closer than anything outside it could be
+            for (int ring = 1;; ring++) {
+                cand.clear();
+                for (int y = std::max(0, cy - ring); y <= std::min((int)side - 1, cy + ring); y++)
+                    for (int x = std::max(0, cx - ring); x <= std::min((int)side - 1, cx + ring); x++) {
+                        const uint32_t c = (uint32_t)y * side + (uint32_t)x;
+                        for (uint32_t q = cell_start[c]; q < cell_start[c + 1]; q++) {
+                            const uint32_t j = cell_pts[q];
+                            if (j == i)
+                                continue;
+                            const double dx = px[i] - px[j], dy = py[i] - py[j];
+                            cand.emplace_back(dx * dx + dy * dy, j);
+                        }
+                    }
+                const bool all = ring >= (int)side;
+                if (cand.size() < k && !all)
+                    continue;
+                std::partial_sort(cand.begin(), cand.begin() + std::min<size_t>(k, cand.size()), cand.end());
+                const double reach = (double)ring / side;  // every point closer than this was searched
+                if (all || cand[k - 1].first < reach * reach)
+                    break;
+            }
+            for (uint32_t t = 0; t < k; t++) {
+                const uint32_t j = cand[t].second;
+                const uint32_t a = (uint32_t)i < j ? (uint32_t)i : j, b = (uint32_t)i < j ? j : (uint32_t)i;
+                pairs[i * k + t] = ((uint64_t)a << 32) | b;
+            }
+        }
+    });
+    std::sort(pairs.begin(), pairs.end());
+    pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+    *out_m = pairs.size();
+    if (out)
+        std::copy(pairs.begin(), pairs.end(), out);
+    if (w)
+        for (uint64_t e = 0; e < pairs.size(); e++) {
+            const uint32_t a = (uint32_t)(pairs[e] >> 32), b = (uint32_t)pairs[e];
+            const double dx = px[a] - px[b], dy = py[a] - py[b];
+            w[e] = (uint32_t)std::floor(std::sqrt(dx * dx + dy * dy) * 16777216.0);
+        }
     return PHEM_OK;
 }
 

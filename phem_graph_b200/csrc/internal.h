@@ -15,7 +15,7 @@ namespace phem {
 // Kernels the library launches; the profile reports them by these names.
 enum KernelId : int {
     kKInit = 0, kKSelect, kKEdgePass, kKHook, kKCompress, kKAdvance, kKGather,
-    kKCcInit, kKCcUnite, kKCcMerge, kKCcLabel, kKMinid, kKCcCount, kKCsrCoo, kKPack,
+    kKCcInit, kKCcUnite, kKCcMerge, kKCcLabel, kKMinid, kKCcCount, kKCsrCoo, kKPack, kKBatch,
     kKernelCount
 };
 extern const char *const kKernelNames[kKernelCount];
@@ -51,6 +51,9 @@ struct phem_context {
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
     int tune_first_batch = 8;            // Boruvka rounds queued before the first host check
     int tune_next_batch = 4;             // rounds queued per later check
+    int tune_batch_block = 512;          // batched kernel: threads per CTA
+    int tune_batch_items = 2;            // batched kernel: records per thread per step
+    double tune_batch_compact = 0.5;     // batched kernel: compaction threshold
     // launch accounting and optional per-kernel CUDA-event timing
     uint64_t launches[phem::kKernelCount] = {};
     double kernel_ms[phem::kKernelCount] = {};
@@ -122,6 +125,96 @@ struct KernelScope {
 };
 // Folds finished event pairs into the per-kernel totals (call after a sync).
 void resolve_timings(phem_context *ctx);
+
+// ---- call helpers shared by the entry points ----
+
+// Makes ctx->device current for the duration of a call, restoring the caller's.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+            prev = -1;
+        if (prev != dev)
+            ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev)
+            cudaSetDevice(prev);
+    }
+};
+
+// A caller array staged through the workspace when it is host memory.
+struct Staged {
+    void *dev = nullptr;   // pointer the kernels use
+    void *host = nullptr;  // caller's host pointer (null when it was already device memory)
+    size_t bytes = 0;
+};
+
+inline phem_status check_ctx(phem_context *ctx)
+{
+    if (!ctx) {
+        set_error("null context");
+        return PHEM_ERR_INVALID;
+    }
+    return PHEM_OK;
+}
+
+// Event-timed region on the context stream.
+struct Timed {
+    phem_context *ctx;
+    explicit Timed(phem_context *c) : ctx(c) { cudaEventRecord(ctx->ev_start, ctx->stream); }
+    float stop()
+    {
+        float ms = 0.f;
+        cudaEventRecord(ctx->ev_stop, ctx->stream);
+        if (cudaEventSynchronize(ctx->ev_stop) == cudaSuccess)
+            cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+        return ms;
+    }
+};
+
+// Stages `bytes` of a caller input into the workspace at `off` when it is host
+// memory (queued on the context stream).
+inline phem_status stage_in(phem_context *ctx, const void *p, size_t bytes, size_t off, Staged *st)
+{
+    st->bytes = bytes;
+    if (is_device_ptr(p)) {
+        st->dev = const_cast<void *>(p);
+        st->host = nullptr;
+        return PHEM_OK;
+    }
+    st->dev = static_cast<char *>(ctx->ws) + off;
+    st->host = nullptr;
+    if (bytes)
+        PHEM_CUDA_TRY(cudaMemcpyAsync(st->dev, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return PHEM_OK;
+}
+
+// An output: device pointer used directly, host pointer via workspace at `off`.
+inline void stage_out(phem_context *ctx, void *p, size_t bytes, size_t off, Staged *st)
+{
+    st->bytes = bytes;
+    if (!p || is_device_ptr(p)) {
+        st->dev = p;
+        st->host = nullptr;
+        return;
+    }
+    st->dev = static_cast<char *>(ctx->ws) + off;
+    st->host = p;
+}
+
+inline phem_status copy_back(phem_context *ctx, const Staged &st, size_t bytes)
+{
+    if (st.host && bytes)
+        PHEM_CUDA_TRY(cudaMemcpyAsync(st.host, st.dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return PHEM_OK;
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // ---- MSF engine (msf.cu) ----
 enum EdgeKind : int { kKindMsf = 0, kKindPacked = 1 };

@@ -512,8 +512,10 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
             const uint64_t i = i0 + q * kBlock + threadIdx.x;
             rec[q] = i < len ? __ldcg(wl + i) : make_uint4(0, 0, 0, 0);
             const bool real = rec[q].x != rec[q].y;
-            ka[q] = real ? __ldcg(a.best + rec[q].x) : 0ull;
-            kb[q] = real ? __ldcg(a.best + rec[q].y) : 0ull;
+            // best is read-only during this kernel: cached loads let the
+            // few hub components of late rounds hit in L1
+            ka[q] = real ? __ldg(a.best + rec[q].x) : 0ull;
+            kb[q] = real ? __ldg(a.best + rec[q].y) : 0ull;
         }
 #pragma unroll
         for (int q = 0; q < 4; q++) {

@@ -90,3 +90,102 @@ def rmat_graph(scale: int, edge_factor: int = 16, seed: int = 22, weight_seed: i
     pairs = rmat(scale, edge_factor * n, seed)
     ws = seed + 1000 if weight_seed is None else weight_seed
     return Graph(f"rmat{scale}_ef{edge_factor}_s{seed}", n, pairs, weights(len(pairs), ws, bits))
+
+
+def rgg(n: int, k: int, seed: int):
+    """2-D random geometric k-nearest-neighbour graph: (pairs, weights), pairs
+    packed (min << 32 | max) and sorted, weights floor(distance * 2^24)."""
+    cap = max(n * k, 1)
+    out = np.empty(cap, np.uint64)
+    w = np.empty(cap, np.uint32)
+    m = C.c_uint64()
+    check(lib().phem_gen_rgg(n, k, seed, out.ctypes.data, w.ctypes.data, C.byref(m)), "phem_gen_rgg")
+    return out[: m.value], w[: m.value]
+
+
+def rgg_graph(n: int, k: int = 8, seed: int = 1) -> Graph:
+    pairs, w = rgg(n, k, seed)
+    return Graph(f"rgg_n{n}_k{k}_s{seed}", n, pairs, w)
+
+
+# ------------------------------------------------------------------ batches
+
+PHEM_BATCH_MSF = 0
+PHEM_BATCH_CC = 1
+
+# phem_batch_graph (include/phem.h)
+BATCH_GRAPH = np.dtype([("edge_offset", "<u8"), ("num_edges", "<u4"), ("num_vertices", "<u4"),
+                        ("vertex_offset", "<u4"), ("kind", "<u4")])
+assert BATCH_GRAPH.itemsize == 24
+
+
+@dataclass
+class Batch:
+    graphs: np.ndarray   # BATCH_GRAPH records
+    edges: np.ndarray    # (E, 3) uint32 {u, v, w}, vertex ids local to each graph
+    total_vertices: int
+    names: list
+
+    @property
+    def num_graphs(self) -> int:
+        return len(self.graphs)
+
+    @property
+    def total_edges(self) -> int:
+        return len(self.edges)
+
+    def graph_edges(self, g: int) -> np.ndarray:
+        r = self.graphs[g]
+        o = int(r["edge_offset"])
+        return self.edges[o: o + int(r["num_edges"])]
+
+
+def batch_from(parts) -> Batch:
+    """Concatenates (name, n, edges (m, 3) uint32, kind) tuples into one batch."""
+    parts = list(parts)
+    graphs = np.zeros(len(parts), BATCH_GRAPH)
+    e_off = v_off = 0
+    for g, (_, n, e, kind) in enumerate(parts):
+        graphs[g] = (e_off, len(e), n, v_off, kind)
+        e_off += len(e)
+        v_off += n
+    edges = np.concatenate([p[2].reshape(-1, 3) for p in parts]) if parts else np.empty((0, 3), np.uint32)
+    return Batch(graphs, np.ascontiguousarray(edges, np.uint32), v_off, [p[0] for p in parts])
+
+
+_TAG_BATCH = 0x42415443482D47  # "BATCH-G"
+
+
+def _unit(seed: int, i: int) -> float:
+    return (int(lib().phem_gen_mix64(seed, _TAG_BATCH, i)) >> 11) * 2.0 ** -53
+
+
+def mixed_graph(i: int, seed: int, n_lo: int = 64, n_hi: int = 65536):
+    """Graph i of the many-small-graphs workload: n log-uniform in [n_lo, n_hi];
+    even i Erdos-Renyi with mean degree uniform in [2, 16] and weights uniform
+    in [1, 2^20], odd i a 2-D random geometric 8-nearest-neighbour graph with
+    weights floor(distance * 2^24)."""
+    n = int(n_lo * (n_hi / n_lo) ** _unit(seed, 4 * i))
+    n = max(n_lo, min(n, n_hi))
+    gs = seed * 1000003 + i
+    if i % 2 == 0:
+        deg = 2.0 + 14.0 * _unit(seed, 4 * i + 1)
+        pairs = er(n, int(round(n * deg / 2)), gs)
+        w = weights(len(pairs), gs + 7)
+        name = f"er{i}_n{n}"
+    else:
+        pairs, w = rgg(n, 8, gs)
+        name = f"rgg{i}_n{n}"
+    return name, n, msf_edges(pairs, w)
+
+
+def mixed_batch(num_graphs: int = 4096, seed: int = 4, n_lo: int = 64, n_hi: int = 65536, kind=PHEM_BATCH_MSF,
+                threads: int = 16) -> Batch:
+    """The many-small-graphs workload (4096 graphs by default); graphs are
+    generated on `threads` host threads (the generators release the GIL).
+    `kind` is a batch kind or a function of the graph index."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(threads) as ex:
+        parts = list(ex.map(lambda i: mixed_graph(i, seed, n_lo, n_hi), range(num_graphs)))
+    kinds = kind if callable(kind) else (lambda i: kind)
+    return batch_from((name, n, e, kinds(i)) for i, (name, n, e) in enumerate(parts))

@@ -90,3 +90,40 @@ def test_msf_edges_records():
     assert E.shape == (len(p), 3)
     np.testing.assert_array_equal(E[:, 0].astype(np.uint64), p >> np.uint64(32))
     np.testing.assert_array_equal(E[:, 2], w)
+
+
+def _rgg_points(n, seed):
+    from phem_graph_b200._lib import lib
+    tag = 0x5247472D505453  # stream tag of the geometric generator
+    raw = np.array([lib().phem_gen_mix64(seed, tag, i) for i in range(2 * n)], np.uint64)
+    xy = (raw >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    return xy[0::2], xy[1::2]
+
+
+@pytest.mark.parametrize("n,k,seed", [(300, 8, 1), (1000, 8, 7), (64, 3, 2)])
+def test_rgg_matches_brute_force_knn(n, k, seed):
+    pairs, w = gen.rgg(n, k, seed)
+    x, y = _rgg_points(n, seed)
+    d2 = (x[:, None] - x[None, :]) ** 2 + (y[:, None] - y[None, :]) ** 2
+    want = set()
+    for i in range(n):
+        for _, j in sorted((d2[i, j], j) for j in range(n) if j != i)[:k]:
+            want.add((min(i, j) << 32) | max(i, j))
+    assert sorted(want) == [int(p) for p in pairs]
+    u = (pairs >> np.uint64(32)).astype(np.int64)
+    v = (pairs & np.uint64(0xFFFFFFFF)).astype(np.int64)
+    np.testing.assert_array_equal(w, np.floor(np.sqrt(d2[u, v]) * 16777216.0).astype(np.uint32))
+
+
+def test_mixed_batch_layout_and_determinism():
+    a = gen.mixed_batch(40, 5, threads=4)
+    b = gen.mixed_batch(40, 5, threads=2)
+    np.testing.assert_array_equal(a.edges, b.edges)
+    np.testing.assert_array_equal(a.graphs, b.graphs)
+    g = a.graphs
+    assert np.all(g["edge_offset"][1:] == g["edge_offset"][:-1] + g["num_edges"][:-1])
+    assert np.all(g["vertex_offset"][1:] == g["vertex_offset"][:-1] + g["num_vertices"][:-1])
+    assert np.all((g["num_vertices"] >= 64) & (g["num_vertices"] <= 65536))
+    for i in range(a.num_graphs):
+        e = a.graph_edges(i)
+        assert np.all(e[:, :2] < int(g["num_vertices"][i])) and np.all(e[:, 0] < e[:, 1])
