@@ -354,6 +354,70 @@ phem_status phem_batch_autotune(phem_context *ctx, const phem_batch_graph *graph
                                 const phem_edge *edges, uint64_t total_edges, uint32_t total_vertices,
                                 uint32_t reps, phem_batch_stats *best);
 
+/* ------------------------------------------------------------------ serving loop */
+/* A request loop with continuous batching.  No reference counterpart (the
+ * reference solves one graph per process run, CC/main.cu, MST/main.cu).
+ * Requests of mixed sizes are submitted from any host thread.  Small ones are
+ * packed into batched persistent launches, `slots` of them in flight at once,
+ * so requests arriving while a batch runs form the next one and start as
+ * soon as a slot frees up; large ones run on the device-wide engines
+ * (phem_msf_solve, phem_cc_solve) in `large_workers` threads, concurrently.
+ * Device memory is bounded by `memory_budget`: slot arenas are fixed at
+ * creation and each device-wide worker grows its workspace at most to its
+ * share; a request that fits nowhere is refused at submission with
+ * PHEM_ERR_NOMEM.  A request's result is the same whichever path serves it
+ * and whatever else is in flight. */
+typedef struct phem_server phem_server;
+
+typedef struct phem_server_config {
+    uint64_t memory_budget;     /* device bytes the server may hold */
+    uint32_t slots;             /* batched launches in flight, 1..8 */
+    uint32_t max_batch_graphs;  /* requests per batched launch */
+    uint64_t large_edges;       /* requests with more edges use the device-wide engines */
+    uint32_t large_workers;     /* concurrent device-wide solves, 1..8 */
+    uint32_t reserved;
+} phem_server_config;
+
+/* One request.  Arrays are host memory owned by the caller and must stay
+ * valid until the request's result has been collected. */
+typedef struct phem_request {
+    uint32_t kind;             /* PHEM_BATCH_MSF or PHEM_BATCH_CC */
+    uint32_t num_vertices;     /* n > 0 */
+    uint64_t num_edges;        /* m */
+    const phem_edge *edges;    /* MSF input: {u, v, w} records */
+    const uint64_t *pairs;     /* CC input: packed (u << 32 | v); pairs with u >= v are skipped */
+    phem_edge *forest;         /* MSF output: forest records ascending by edge index
+                                  (room for n - 1; may be NULL) */
+    int32_t *labels;           /* CC output: min-id labels, n entries (may be NULL) */
+} phem_request;
+
+#define PHEM_PATH_BATCHED 0u
+#define PHEM_PATH_DEVICE 1u
+
+typedef struct phem_request_result {
+    int32_t status;            /* phem_status of this request */
+    uint32_t path;             /* PHEM_PATH_BATCHED or PHEM_PATH_DEVICE */
+    uint64_t forest_edges;     /* forest size (CC: n - components) */
+    uint64_t total_weight;     /* MSF: uint64 forest weight; CC: 0 */
+    uint64_t submit_ns;        /* steady-clock times: submitted, work started, result written */
+    uint64_t start_ns;
+    uint64_t done_ns;
+} phem_request_result;
+
+phem_status phem_server_create(int device, const phem_server_config *cfg, phem_server **out);
+/* Finishes every submitted request, then releases the server. */
+void phem_server_destroy(phem_server *server);
+/* Queues a request (thread-safe); *ticket identifies it for phem_server_wait. */
+phem_status phem_server_submit(phem_server *server, const phem_request *req, uint64_t *ticket);
+/* Waits for a request (timeout_ms 0: no limit) and returns its result; each
+ * ticket is collected once. */
+phem_status phem_server_wait(phem_server *server, uint64_t ticket, uint32_t timeout_ms, phem_request_result *res);
+/* Open-loop load: submits reqs[i] at arrival_ns[i] after the call starts
+ * (nanoseconds, non-decreasing), then collects every result in order.
+ * Returns the first submission error (results[i].status has each one). */
+phem_status phem_server_replay(phem_server *server, const phem_request *reqs, const uint64_t *arrival_ns,
+                               uint32_t count, phem_request_result *results);
+
 /* --------------------------------------------------------- synthetic inputs (host) */
 /* Seeded generators for tests and benchmarks (no reference counterpart: the
  * reference reads graph files).  Deterministic for any thread count. */

@@ -28,6 +28,8 @@ PHEM_CC_CANONICAL = 1
 PHEM_CC_NOALLOC_MAX_VERTICES = 1 << 20
 PHEM_BATCH_MSF = 0
 PHEM_BATCH_CC = 1
+PHEM_PATH_BATCHED = 0
+PHEM_PATH_DEVICE = 1
 
 
 class PhemError(RuntimeError):
@@ -64,6 +66,22 @@ class LaunchRecord(C.Structure):
 class BatchGraph(C.Structure):
     _fields_ = [("edge_offset", C.c_uint64), ("num_edges", C.c_uint32), ("num_vertices", C.c_uint32),
                 ("vertex_offset", C.c_uint32), ("kind", C.c_uint32)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("memory_budget", C.c_uint64), ("slots", C.c_uint32), ("max_batch_graphs", C.c_uint32),
+                ("large_edges", C.c_uint64), ("large_workers", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("num_vertices", C.c_uint32), ("num_edges", C.c_uint64),
+                ("edges", C.c_void_p), ("pairs", C.c_void_p), ("forest", C.c_void_p), ("labels", C.c_void_p)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("path", C.c_uint32), ("forest_edges", C.c_uint64),
+                ("total_weight", C.c_uint64), ("submit_ns", C.c_uint64), ("start_ns", C.c_uint64),
+                ("done_ns", C.c_uint64)]
 
 
 class BatchStats(C.Structure):
@@ -125,6 +143,11 @@ SIGNATURES = {
                                          C.POINTER(_VP)]),
     "phem_batch_autotune": (C.c_int, [_VP, _VP, C.c_uint32, _VP, C.c_uint64, C.c_uint32, C.c_uint32,
                                       C.POINTER(BatchStats)]),
+    "phem_server_create": (C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_VP)]),
+    "phem_server_destroy": (None, [_VP]),
+    "phem_server_submit": (C.c_int, [_VP, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "phem_server_wait": (C.c_int, [_VP, C.c_uint64, C.c_uint32, C.POINTER(RequestResult)]),
+    "phem_server_replay": (C.c_int, [_VP, C.POINTER(Request), _VP, C.c_uint32, C.POINTER(RequestResult)]),
 }
 
 

@@ -82,13 +82,34 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t x, ScanSmem<B> &s, int p
 
 __device__ __forceinline__ unsigned long long graph_key(uint32_t kind, uint32_t w, uint32_t id)
 {
-    return kind == PHEM_BATCH_CC ? (unsigned long long)id : (((unsigned long long)w << 32) | id);
+    return kind == PHEM_BATCH_MSF ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
 }
 
 __device__ __forceinline__ void offer(unsigned long long *best, uint32_t t, unsigned long long key)
 {
     if (key < *(volatile unsigned long long *)(best + t))
         atomicMin(best + t, key);
+}
+
+// Input record i of a graph: {u, v, w} records, or packed CC pairs
+// (u << 32 | v) when p0 is set; a pair with u >= v is skipped, as the
+// reference's union kernel skips it (CC/ExternalSpanningTree.cu:82), by
+// turning it into a self-loop.
+__device__ __forceinline__ void load_edge(const phem_edge *e0, const unsigned long long *p0, uint32_t i, uint32_t &u,
+                                          uint32_t &v, uint32_t &w)
+{
+    if (p0) {
+        const unsigned long long p = __ldg(p0 + i);
+        u = (uint32_t)(p >> 32);
+        v = (uint32_t)p;
+        w = 0;
+        if (u >= v)
+            u = v = 0;  // skipped whatever its range, as the reference skips it
+    } else {
+        u = __ldg(&e0[i].u);
+        v = __ldg(&e0[i].v);
+        w = __ldg(&e0[i].w);
+    }
 }
 
 template <int B>
@@ -106,7 +127,8 @@ struct BatchSmem {
 // of its own slots, and all its reads precede the scan barrier).  Returns the
 // survivor count; *len_out gets the new list length.
 template <int B, int I, bool FIRST>
-__device__ uint32_t relabel_pass(const phem_edge *e0, uint4 *wl, uint32_t len, bool compact, uint32_t n,
+__device__ uint32_t relabel_pass(const phem_edge *e0, const unsigned long long *p0, uint4 *wl, uint32_t len,
+                                 bool compact, uint32_t n,
                                  uint32_t kind, const uint32_t *comp, unsigned long long *best,
                                  BatchSmem<B> &sm, uint32_t *len_out)
 {
@@ -122,7 +144,8 @@ __device__ uint32_t relabel_pass(const phem_edge *e0, uint4 *wl, uint32_t len, b
             rec[j] = make_uint4(0, 0, 0, 0);
             if (i < len) {
                 if (FIRST) {
-                    const uint32_t u = __ldg(&e0[i].u), v = __ldg(&e0[i].v), w = __ldg(&e0[i].w);
+                    uint32_t u, v, w;
+                    load_edge(e0, p0, i, u, v, w);
                     if (u >= n || v >= n) {
                         atomicOr(&sm.err, kErrRange);
                     } else if (u != v) {
@@ -169,6 +192,7 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
 {
     const uint32_t n = it.n, m = it.m;
     const phem_edge *e0 = a.edges + it.e_off;
+    const unsigned long long *p0 = it.kind == kBatchPairs ? a.pairs + it.e_off : nullptr;
     uint4 *wl = a.wl + it.wl_off;
     uint32_t *bm = a.bitmap + it.bm_off;
     const bool local = n <= a.smem_vertices;
@@ -188,7 +212,7 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
     __syncthreads();
 
     uint32_t len = 0;
-    uint32_t live = relabel_pass<B, I, true>(e0, wl, m, true, n, it.kind, comp, best, sm, &len);
+    uint32_t live = relabel_pass<B, I, true>(e0, p0, wl, m, true, n, it.kind, comp, best, sm, &len);
     uint32_t rounds = 0;
     while (live > 0) {
         if (++rounds > kBatchMaxRounds) {
@@ -203,7 +227,9 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
             if (k == kKeyInf)
                 continue;
             const uint32_t id = (uint32_t)k;
-            const uint32_t cu = comp[__ldg(&e0[id].u)], cv = comp[__ldg(&e0[id].v)];
+            uint32_t eu, ev, ew;
+            load_edge(e0, p0, id, eu, ev, ew);
+            const uint32_t cu = comp[eu], cv = comp[ev];
             const uint32_t other = cu == x ? cv : cu;
             if (best[other] == k && x < other)
                 continue;  // mutual pair: the lower root stays a root
@@ -229,7 +255,7 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
         }
         __syncthreads();
         const bool compact = (float)live <= a.compact_ratio * (float)len;
-        live = relabel_pass<B, I, false>(e0, wl, len, compact, n, it.kind, comp, best, sm, &len);
+        live = relabel_pass<B, I, false>(e0, p0, wl, len, compact, n, it.kind, comp, best, sm, &len);
     }
     __syncthreads();
 
@@ -262,7 +288,7 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
             else
                 atomicOr(&sm.err, kErrCapacity);
             pos++;
-            if (it.kind != PHEM_BATCH_CC)
+            if (it.kind == PHEM_BATCH_MSF)
                 wsum += __ldg(&e0[id].w);
         }
         out += total;

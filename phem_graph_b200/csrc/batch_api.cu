@@ -7,16 +7,6 @@
 #include "batch.h"
 
 namespace phem {
-namespace {
-
-// Validated work items in queue order (largest graphs first, so the longest
-// solves start early and the persistent grid finishes together), with the
-// private scratch offsets of every graph.
-struct BatchLayout {
-    std::vector<BatchItem> items;
-    uint64_t wl_records = 0;
-    uint64_t bm_words = 0;
-};
 
 phem_status build_items(const phem_batch_graph *graphs, uint32_t G, uint64_t total_edges, uint32_t total_vertices,
                         BatchLayout *L)
@@ -91,20 +81,6 @@ phem_status build_items(const phem_batch_graph *graphs, uint32_t G, uint64_t tot
     return PHEM_OK;
 }
 
-// Device buffers of one batch (context workspace or plan memory).
-struct BatchBuffers {
-    BatchItem *items;
-    uint32_t *num_graphs, *queue;
-    phem_edge *edges;
-    uint4 *wl;
-    uint32_t *bitmap, *g_parent, *g_comp;
-    unsigned long long *g_best;
-    uint32_t *msf_ids, *msf_count;
-    unsigned long long *msf_total;
-    int32_t *labels;
-    uint32_t *status, *rounds;
-};
-
 // Carves every buffer for the given capacities out of `base` (null: sizing
 // only); returns the bytes needed.  `edges_inline` is false when the
 // caller's device edges are used in place.
@@ -162,6 +138,8 @@ BatchArgs make_args(const BatchBuffers &b, const phem_edge *edges, float ratio)
     a.compact_ratio = ratio;
     return a;
 }
+
+namespace {
 
 phem_status batch_status(const uint32_t *status, uint32_t G)
 {
@@ -225,22 +203,50 @@ void fill_stats(phem_batch_stats *st, const BatchLaunch &l, float ratio, float m
 
 using namespace phem;
 
-struct phem_batch_plan {
-    phem_context *ctx = nullptr;
-    uint32_t max_graphs = 0, max_vertices = 0;
-    uint64_t max_edges = 0, max_wl = 0, max_bm = 0;
-    void *mem = nullptr;
-    BatchBuffers buf{};
-    BatchLaunch launch{};
-    float ratio = 0.5f;
-    BatchItem *h_items = nullptr;  // pinned staging of the work items
-    uint32_t *h_num = nullptr;     // pinned batch size
-    uint32_t *h_status = nullptr;  // pinned per-graph status
-    cudaEvent_t staged = nullptr;  // the pinned staging has been consumed
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    uint32_t num_graphs = 0, total_vertices = 0;
-};
+namespace phem {
+
+// (Re)captures a plan's launch -- queue reset + persistent kernel -- into its
+// CUDA graph, with `pairs` as the input of kBatchPairs graphs.
+phem_status batch_plan_capture(phem_batch_plan *p, const unsigned long long *pairs)
+{
+    if (p->exec) {
+        cudaGraphExecDestroy(p->exec);
+        p->exec = nullptr;
+    }
+    if (p->graph) {
+        cudaGraphDestroy(p->graph);
+        p->graph = nullptr;
+    }
+    *p->h_num = 0;
+    cudaStream_t s = p->ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(p->buf.num_graphs, p->h_num, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess)
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        const cudaError_t e1 = cudaMemsetAsync(p->buf.queue, 0, sizeof(uint32_t), s);
+        BatchArgs a = make_args(p->buf, p->buf.edges, p->ratio);
+        a.pairs = pairs;
+        a.smem_vertices = p->launch.smem_vertices;
+        void *params[] = {&a};
+        const cudaError_t e2 = cudaLaunchKernel(p->launch.kernel, dim3(p->launch.grid), dim3(p->launch.block),
+                                                params, p->launch.dyn_smem, s);
+        e = cudaStreamEndCapture(s, &p->graph);
+        if (e == cudaSuccess)
+            e = e1 != cudaSuccess ? e1 : e2;
+    }
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    if (e != cudaSuccess) {
+        set_error("batch plan: graph capture failed: %s", cudaGetErrorString(e));
+        cudaGetLastError();
+        return PHEM_ERR_CUDA;
+    }
+    return PHEM_OK;
+}
+
+}  // namespace phem
 
 extern "C" {
 
@@ -414,31 +420,7 @@ phem_status phem_batch_plan_create(phem_context *ctx, uint32_t max_graphs, uint6
     if (st == PHEM_OK) {
         batch_carve(max_graphs, max_edges, p->max_wl, p->max_bm, max_vertices, true, static_cast<char *>(p->mem),
                     &p->buf);
-        *p->h_num = 0;
-        cudaStream_t s = ctx->stream;
-        cudaError_t e = cudaMemcpyAsync(p->buf.num_graphs, p->h_num, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess)
-            e = cudaStreamSynchronize(s);
-        if (e == cudaSuccess)
-            e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            cudaError_t e1 = cudaMemsetAsync(p->buf.queue, 0, sizeof(uint32_t), s);
-            BatchArgs a = make_args(p->buf, p->buf.edges, p->ratio);
-            a.smem_vertices = p->launch.smem_vertices;
-            void *params[] = {&a};
-            cudaError_t e2 = cudaLaunchKernel(p->launch.kernel, dim3(p->launch.grid), dim3(p->launch.block), params,
-                                              p->launch.dyn_smem, s);
-            e = cudaStreamEndCapture(s, &p->graph);
-            if (e == cudaSuccess)
-                e = e1 != cudaSuccess ? e1 : e2;
-        }
-        if (e == cudaSuccess)
-            e = cudaGraphInstantiate(&p->exec, p->graph, 0);
-        if (e != cudaSuccess) {
-            set_error("batch_plan_create: graph capture failed: %s", cudaGetErrorString(e));
-            cudaGetLastError();
-            st = PHEM_ERR_CUDA;
-        }
+        st = phem::batch_plan_capture(p, nullptr);
     }
     if (st != PHEM_OK) {
         phem_batch_plan_destroy(p);
