@@ -18,6 +18,13 @@ Workload (one "step" = one full minimum-spanning-forest solve):
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl phem|reference]
 
+On one GPU the same JSON line also carries the metric's other workloads:
+  cc       connected components + forest, Erdos-Renyi n = 2^20, 8 * 2^20 draws;
+  batched  4096 small graphs (ER and geometric) in one persistent launch,
+           against one solve per graph;
+  served   Poisson request streams at 1k-100k req/s through the serving loop
+           (p50 / p99 latency, throughput), against serial one-graph solves.
+
 Multi-GPU (torchrun, one rank per GPU): every rank solves its own shard of a
 global multigraph (same vertex set, seed 22 + rank, 2^26 draws each), the local
 forests are all-gathered over NCCL and every rank solves their union; value =
@@ -175,6 +182,179 @@ def cpu_baseline_pbbs(E: np.ndarray, budget_s: float = 20.0, max_runs: int = 5) 
             "seconds_median": med}
 
 
+def bench_cc(ctx, torch, peaks: dict, steps: int, warmup: int, cpu: bool) -> dict:
+    """Connected components + spanning forest on Erdos-Renyi n = 2^20 with
+    8 * 2^20 uniform draws (seed 1; self-loops dropped, duplicates kept):
+    device time of phem_cc_solve on resident packed edges (CUDA events around
+    init + union + label), the algorithmic bytes 8 m + 16 n against the
+    measured HBM bandwidth, end to end from pinned host pairs to host labels,
+    and the reference's host_spanning_tree on the host cores."""
+    from phem_graph_b200 import gen
+    g = gen.er_graph(1 << 20, 8 << 20, 1)
+    n, m = g.n, g.m
+    dev = torch.device("cuda", ctx.device)
+    d_pairs = torch.from_numpy(g.pairs.view(np.int64)).to(dev)
+    d_lab = torch.empty(n, dtype=torch.int32, device=dev)
+    d_for = torch.empty(n, dtype=torch.int64, device=dev)
+    out = {}
+    for name, canon in (("default", False), ("canonical", True)):
+        for _ in range(warmup):
+            ctx.cc_solve(d_pairs, n, canonical=canon, labels=d_lab, forest=d_for)
+        ms = [ctx.cc_solve(d_pairs, n, canonical=canon, labels=d_lab, forest=d_for).device_ms for _ in range(steps)]
+        t = statistics.median(ms)
+        byts = 8 * m + 16 * n
+        out[name] = {"value": m / (t / 1e3) / 1e9, "ms": t, "algorithmic_bytes": byts,
+                     "achieved_gbs": byts / (t / 1e3) / 1e9, "frac": byts / (t / 1e3) / 1e9 / peaks["hbm_gbs"]}
+    h_pairs = torch.from_numpy(g.pairs.view(np.int64)).pin_memory()
+    h_lab = torch.empty(n, dtype=torch.int32).pin_memory()
+    hp, hl = h_pairs.numpy().view(np.uint64), h_lab.numpy()
+    ctx.cc_solve(hp, n, labels=hl, want_forest=False)
+    t0 = time.perf_counter()
+    reps = max(3, steps // 2)
+    for _ in range(reps):
+        r = ctx.cc_solve(hp, n, labels=hl, want_forest=False)
+    e2e = (time.perf_counter() - t0) / reps
+    line = {"workload": "cc_er_n2^20_d8x2^20_s1", "n": n, "m": m, "unit": UNIT, "components": r.components,
+            "value": out["default"]["value"], "ms_per_solve": out["default"]["ms"],
+            "roofline": {"bound": "hbm", "achieved": out["default"]["achieved_gbs"], "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": out["default"]["frac"], "bytes_model": "8 m + 16 n"},
+            "canonical_forest": out["canonical"],
+            "e2e": {"value": m / e2e / 1e9, "unit": UNIT, "ms_per_step": e2e * 1e3, "h2d_bytes_per_step": 8 * m,
+                    "d2h_bytes_per_step": 4 * n, "api": "phem_cc_solve (C ABI), pinned host pairs"}}
+    if cpu:
+        import oracle
+        if oracle.ref_available():
+            ref = oracle.RefCC(n)
+            ref.set_edges(g.pairs)
+            ref.run()
+            times = []
+            for _ in range(3):
+                ref.reset()
+                times.append(ref.run())
+            line["cpu_baseline"] = {"value": m / statistics.median(times) / 1e9, "unit": UNIT,
+                                    "cores": ref.workers(), "kind": "reference",
+                                    "sample": "host_spanning_tree (CC/host_spanning_tree.cu) on the full edge list, "
+                                              "median of 3 after 1 warm-up, call time only"}
+            ref.close()
+    return line
+
+
+def bench_batched(ctx, torch, num_graphs: int = 4096) -> dict:
+    """Many small graphs: 4096 graphs, n log-uniform in [64, 65536], half
+    Erdos-Renyi (mean degree U[2, 16], weights U[1, 2^20]), half 2-D random
+    geometric 8-NN (weights floor(distance * 2^24)), every graph solved for
+    MSF + labels.  The autotuner picks the kernel configuration, then the
+    captured launch is replayed (CUDA events); the one-solve-per-launch path
+    (phem_msf_solve per graph, inputs resident on the host) is timed on a
+    256-graph sample and scaled to the batch by its share of the edges."""
+    from phem_graph_b200 import gen
+    b = gen.mixed_batch(num_graphs, 4)
+    tuned = ctx.batch_autotune(b, reps=2)
+    dev = torch.device("cuda", ctx.device)
+    with ctx.batch_plan(b.num_graphs, b.total_edges, b.total_vertices) as p:
+        p.upload(b)
+        for _ in range(3):
+            p.run()
+        stream = torch.cuda.ExternalStream(__import__("phem_graph_b200").lib().phem_context_stream(ctx.handle),
+                                           device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        reps = 10
+        e0.record(stream)
+        for _ in range(reps):
+            p.run()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res = p.download(labels=False)
+    # end to end: host batch in, host results out, through phem_batch_solve
+    ctx.batch_solve(b, labels=True)
+    t0 = time.perf_counter()
+    r = ctx.batch_solve(b, labels=True)
+    e2e = time.perf_counter() - t0
+    assert np.array_equal(r.count, res.count) and np.array_equal(r.total, res.total)
+    idx = np.random.default_rng(0).choice(b.num_graphs, 256, replace=False)
+    sample = [(np.ascontiguousarray(b.graph_edges(g)), int(b.graphs[g]["num_vertices"])) for g in idx]
+    for e, n in sample[:8]:
+        ctx.msf_solve(e, n)
+    t0 = time.perf_counter()
+    for e, n in sample:
+        one = ctx.msf_solve(e, n)
+    plain_s = time.perf_counter() - t0
+    frac = sum(len(e) for e, _ in sample) / b.total_edges
+    plain_batch_s = plain_s / frac
+    return {"workload": "batched_4096_mixed_er_rgg", "graphs": b.num_graphs, "edges": b.total_edges,
+            "vertices": b.total_vertices, "unit": UNIT, "value": b.total_edges / (ms / 1e3) / 1e9,
+            "ms_per_batch": ms, "graphs_per_s": b.num_graphs / (ms / 1e3), "launches_per_batch": 1,
+            "config": {k: tuned[k] for k in ("block_size", "items", "compact_ratio", "grid", "smem_vertices")},
+            "replay": "captured CUDA graph (queue reset + persistent kernel)",
+            "one_launch_per_graph": {"value": b.total_edges / plain_batch_s / 1e9, "s_per_batch": plain_batch_s,
+                                     "sample": "256 graphs through phem_msf_solve, scaled by edge share"},
+            "speedup_vs_one_launch_per_graph": plain_batch_s / (ms / 1e3),
+            "e2e": {"value": b.total_edges / e2e / 1e9, "unit": UNIT, "ms_per_step": e2e * 1e3,
+                    "h2d_bytes_per_step": 12 * b.total_edges + 24 * b.num_graphs,
+                    "d2h_bytes_per_step": 8 * b.total_vertices + 12 * b.num_graphs,
+                    "api": "phem_batch_solve (C ABI), host arrays"}}
+
+
+def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), per_rate: int = 256) -> dict:
+    """Served request stream: Poisson arrivals at each rate, requests drawn
+    from a pool of 64 graphs with m log-uniform in [2^10, 2^24] (70% CC packed
+    pairs, 30% MSF records with weights U[1, 2^20]; half Erdos-Renyi, half
+    R-MAT), request buffers in pinned host memory, a 64 GB device budget.
+    Latency = submission to result written to host; throughput = edges of all
+    requests / wall time of the run.  The serial baseline solves the same
+    pool one request at a time through the one-graph entry points."""
+    import phem_graph_b200 as P
+    from phem_graph_b200.serve import PHEM_BATCH_MSF, Server, poisson_arrivals, request_pool
+    pool = request_pool(64, seed=5)
+    keep = []
+    for g in pool:  # pinned request buffers, as a server's receive path would hold them
+        if g.kind == PHEM_BATCH_MSF:
+            t = torch.from_numpy(g.edges.view(np.int32)).pin_memory()
+            keep.append(t)
+            g.edges = t.numpy().view(np.uint32)
+        else:
+            t = torch.from_numpy(g.pairs.view(np.int64)).pin_memory()
+            keep.append(t)
+            g.pairs = t.numpy().view(np.uint64)
+    ctx = P.Context(0)
+    solve = (lambda g: ctx.msf_solve(g.edges, g.n) if g.kind == PHEM_BATCH_MSF
+             else ctx.cc_solve(g.pairs, g.n, want_forest=False))
+    for g in pool[:4]:
+        solve(g)
+    t0 = time.perf_counter()
+    for g in pool:
+        solve(g)
+    serial_s = time.perf_counter() - t0
+    ctx.close()
+    pool_edges = sum(g.m for g in pool)
+    rng = np.random.default_rng(1)
+    points = []
+    with Server(memory_budget=64 << 30, slots=2, max_batch_graphs=1024, large_edges=1 << 18,
+                large_workers=2) as srv:
+        srv.replay(pool[:8], np.zeros(8, np.uint64))
+        for rate in rates:
+            reqs = [pool[i] for i in rng.integers(0, len(pool), per_rate)]
+            arr = poisson_arrivals(per_rate, rate, seed=rate)
+            t0 = time.perf_counter()
+            res = srv.replay(reqs, arr)
+            wall = time.perf_counter() - t0
+            lat = np.array([s.latency_ns for s in res]) / 1e6
+            assert all(s.status == 0 for s in res)
+            e = sum(g.m for g in reqs)
+            points.append({"rate_req_s": rate, "requests": per_rate, "p50_ms": float(np.percentile(lat, 50)),
+                           "p99_ms": float(np.percentile(lat, 99)), "throughput": e / wall / 1e9,
+                           "req_s": per_rate / wall,
+                           "batched_share": float(np.mean([s.path == 0 for s in res]))})
+    return {"workload": "served_poisson_m_loguniform_2^10_2^24_70cc_30msf", "unit": UNIT, "points": points,
+            "value": max(p["throughput"] for p in points),
+            "serial_plain": {"value": pool_edges / serial_s / 1e9, "req_s": len(pool) / serial_s,
+                             "api": "phem_msf_solve / phem_cc_solve one request at a time, pinned host inputs"},
+            "config": {"memory_budget_gb": 64, "slots": 2, "max_batch_graphs": 1024, "large_edges": 1 << 18,
+                       "large_workers": 2, "pool_graphs": len(pool), "pool_edges": pool_edges}}
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's own CPU path (PBBS mst()) on the same
     workload, all host threads; one step = one full solve."""
@@ -230,6 +410,8 @@ def main() -> None:
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the connected-components, batched and served workloads")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -364,6 +546,13 @@ def main() -> None:
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pbbs(E)
+    if rank == 0 and world == 1 and not args.no_extra:
+        # the other workloads of the metric, measured after the headline run
+        del d_edges, d_out
+        torch.cuda.empty_cache()
+        line["cc"] = bench_cc(ctx, torch, peaks, args.steps, args.warmup, not args.no_cpu_baseline)
+        line["batched"] = bench_batched(ctx, torch)
+        line["served"] = bench_served(torch)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()
