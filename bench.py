@@ -355,6 +355,66 @@ def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), per_rate: int 
                        "large_workers": 2, "pool_graphs": len(pool), "pool_edges": pool_edges}}
 
 
+def bench_streamed(ctx, torch, scale: int, edge_factor: int = 32, batch: int = 1 << 28) -> dict:
+    """Streaming spanning forest (the reference's SpanningTree): R-MAT at
+    `scale` with edge_factor * 2^scale draws (seed 28, self-loops dropped,
+    unsorted, ~69 GB of pairs at scale 28) generated into pinned host memory
+    before timing, then streamed to the GPU in batches of `batch` pairs
+    through triple-buffered copies overlapped with the union kernels
+    (phem_cc_stream); device memory: parent + labels + forest + 3 batch
+    buffers.  Checked by size-independent properties: labels are min-id and
+    idempotent, the forest has n - components edges, and a sample of edges
+    joins equal labels."""
+    from phem_graph_b200 import _lib
+    n = 1 << scale
+    draws = edge_factor << scale
+    h = torch.empty(draws, dtype=torch.int64).pin_memory()
+    base = h.data_ptr()
+    filled, chunk = 0, 1 << 28
+    t_gen = time.perf_counter()
+    for first in range(0, draws, chunk):
+        cnt = __import__("ctypes").c_uint64()
+        _lib.check(_lib.lib().phem_gen_rmat_range(scale, first, min(chunk, draws - first), 0.57, 0.19, 0.19, 28,
+                                                  base + 8 * filled, __import__("ctypes").byref(cnt)),
+                   "phem_gen_rmat_range")
+        filled += cnt.value
+    t_gen = time.perf_counter() - t_gen
+    m = filled
+    dev = torch.device("cuda", ctx.device)
+    parent = torch.empty(n, dtype=torch.int32, device=dev)
+    label = torch.empty(n, dtype=torch.int32, device=dev)
+    forest = torch.empty(n, dtype=torch.int64, device=dev)
+    hv = h[:m].numpy().view(np.uint64)
+    # host link bandwidth for the roofline: one pinned copy of a batch
+    probe = torch.empty(min(batch, m), dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    probe.copy_(h[: probe.numel()], non_blocking=True)
+    torch.cuda.synchronize()
+    h2d_gbs = 8 * probe.numel() / (time.perf_counter() - t0) / 1e9
+    del probe
+    ms = ctx.cc_stream(hv, n, batch, parent, label, forest)
+    ctx.cc_label(n, parent, label)
+    torch.cuda.synchronize()
+    ar = torch.arange(n, dtype=torch.int32, device=dev)
+    lab = label.long()
+    ok_min = bool((label <= ar).all()) and bool((label[lab] == label).all())
+    comps = int((label == ar).sum())
+    filled_slots = int((forest != 0x7FFFFFFF).sum())
+    idx = torch.randint(0, m, (1 << 20,), generator=torch.Generator().manual_seed(0))
+    smp = h[idx].to(dev)
+    su, sv = (smp >> 32).long(), (smp & 0xFFFFFFFF).long()
+    ok_edges = bool((label[su] == label[sv]).all())
+    return {"workload": f"stream_rmat{scale}_ef{edge_factor}_batch2^{batch.bit_length() - 1}", "n": n, "m": m,
+            "unit": UNIT, "value": m / (ms / 1e3) / 1e9, "ms": ms, "generation_s": t_gen,
+            "roofline": {"bound": "host link", "achieved": 8 * m / (ms / 1e3) / 1e9, "peak": h2d_gbs,
+                         "unit": "GB/s", "frac": 8 * m / (ms / 1e3) / 1e9 / h2d_gbs,
+                         "peak_source": "one pinned host-to-device copy of a batch, measured here"},
+            "device_bytes": 16 * n + 3 * 8 * batch, "components": comps,
+            "checks": {"labels_min_id_idempotent": ok_min, "forest_edges_eq_n_minus_c": filled_slots == n - comps,
+                       "sampled_edges_join_equal_labels": ok_edges}}
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's own CPU path (PBBS mst()) on the same
     workload, all host threads; one step = one full solve."""
@@ -410,6 +470,8 @@ def main() -> None:
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stream-scale", type=int, default=0,
+                    help="also stream an R-MAT graph of this scale (edge factor 32) from pinned host memory")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the connected-components, batched and served workloads")
     args = ap.parse_args()
@@ -553,6 +615,8 @@ def main() -> None:
         line["cc"] = bench_cc(ctx, torch, peaks, args.steps, args.warmup, not args.no_cpu_baseline)
         line["batched"] = bench_batched(ctx, torch)
         line["served"] = bench_served(torch)
+    if rank == 0 and world == 1 and args.stream_scale:
+        line["streamed"] = bench_streamed(ctx, torch, args.stream_scale)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()

@@ -438,6 +438,12 @@ phem_status phem_gen_er(uint32_t n, uint64_t draws, uint64_t seed, uint64_t *out
 phem_status phem_gen_rmat(uint32_t scale, uint64_t draws, double a, double b, double c, uint64_t seed,
                           uint64_t *out, uint64_t *out_m);
 
+/* Draws [first, first + count) of the phem_gen_rmat stream, unsorted, packed
+ * (min << 32 | max), self-loops dropped, draw order kept (for generating a
+ * huge graph batch by batch).  out needs `count` entries (NULL to count). */
+phem_status phem_gen_rmat_range(uint32_t scale, uint64_t first, uint64_t count, double a, double b, double c,
+                                uint64_t seed, uint64_t *out, uint64_t *out_m);
+
 /* w[i] = 1 + (SplitMix64 value i & (2^bits - 1)), i.e. uniform in [1, 2^bits]. */
 phem_status phem_gen_weights(uint64_t m, uint64_t seed, uint32_t bits, uint32_t *w);
 

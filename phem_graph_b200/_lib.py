@@ -131,6 +131,8 @@ SIGNATURES = {
     "phem_gen_weights": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, _VP]),
     "phem_pack_msf_edges": (C.c_int, [_VP, _VP, C.c_uint64, _VP]),
     "phem_csr_from_sorted_pairs": (C.c_int, [_VP, C.c_uint64, C.c_uint32, _VP, _VP]),
+    "phem_gen_rmat_range": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                      C.c_uint64, _VP, C.POINTER(C.c_uint64)]),
     "phem_gen_rgg": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, _VP, _VP, C.POINTER(C.c_uint64)]),
     "phem_batch_solve": (C.c_int, [_VP, _VP, C.c_uint32, _VP, C.c_uint64, C.c_uint32, _VP, _VP, _VP, _VP,
                                    C.POINTER(BatchStats)]),

@@ -146,6 +146,39 @@ void radix_sort(uint64_t *keys, uint64_t count, int bits)
         std::memcpy(keys, src, count * sizeof(uint64_t));
 }
 
+// Draw i of an R-MAT stream: `scale` quadrant choices, each from 32 random
+// bits compared against integer thresholds; (lo, hi) with lo < hi, or false
+// for a self-loop.
+struct RmatDraw {
+    uint32_t scale, words;
+    uint64_t base, tA, tAB, tABC;
+    RmatDraw(uint32_t s, double a, double b, double c, uint64_t seed)
+        : scale(s), words((s + 1) / 2), base(stream_base(seed, kTagRMAT))
+    {
+        const double two32 = 4294967296.0;
+        tA = (uint64_t)std::floor(a * two32);
+        tAB = (uint64_t)std::floor((a + b) * two32);
+        tABC = (uint64_t)std::floor((a + b + c) * two32);
+    }
+    bool operator()(uint64_t i, uint32_t *lo, uint32_t *hi) const
+    {
+        uint32_t u = 0, v = 0;
+        for (uint32_t l = 0; l < scale; l++) {
+            const uint64_t word = stream_at(base, i * words + l / 2);
+            const uint64_t r = (l & 1) ? (word >> 32) : (word & 0xffffffffu);
+            const uint32_t ubit = r >= tAB;                          // quadrants c, d
+            const uint32_t vbit = (r >= tA && r < tAB) || r >= tABC;  // quadrants b, d
+            u = (u << 1) | ubit;
+            v = (v << 1) | vbit;
+        }
+        if (u == v)
+            return false;
+        *lo = u < v ? u : v;
+        *hi = u < v ? v : u;
+        return true;
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -177,27 +210,13 @@ phem_status phem_gen_rmat(uint32_t scale, uint64_t draws, double a, double b, do
 {
     if (scale < 1 || scale > 31 || !out_m || a < 0 || b < 0 || c < 0 || a + b + c > 1.0)
         return PHEM_ERR_INVALID;
-    const uint64_t base = stream_base(seed, kTagRMAT);
-    const uint32_t words = (scale + 1) / 2;
-    const double two32 = 4294967296.0;
-    const uint64_t tA = (uint64_t)std::floor(a * two32);
-    const uint64_t tAB = (uint64_t)std::floor((a + b) * two32);
-    const uint64_t tABC = (uint64_t)std::floor((a + b + c) * two32);
+    const RmatDraw draw(scale, a, b, c, seed);
     // Pairs are emitted compactly as (lo << scale | hi) so the sort runs on 2*scale bits.
     uint64_t m = emit_in_draw_order(draws, out, [&](uint64_t i, uint64_t *val) {
-        uint32_t u = 0, v = 0;
-        for (uint32_t l = 0; l < scale; l++) {
-            uint64_t word = stream_at(base, i * words + l / 2);
-            uint64_t r = (l & 1) ? (word >> 32) : (word & 0xffffffffu);
-            uint32_t ubit = r >= tAB;                       // quadrants c, d
-            uint32_t vbit = (r >= tA && r < tAB) || r >= tABC;  // quadrants b, d
-            u = (u << 1) | ubit;
-            v = (v << 1) | vbit;
-        }
-        if (u == v)
+        uint32_t lo, hi;
+        if (!draw(i, &lo, &hi))
             return false;
-        uint64_t lo = u < v ? u : v, hi = u < v ? v : u;
-        *val = (lo << scale) | hi;
+        *val = ((uint64_t)lo << scale) | hi;
         return true;
     });
     if (out) {
@@ -269,6 +288,25 @@ phem_status phem_csr_from_sorted_pairs(const uint64_t *pairs, uint64_t m, uint32
         cols[lowpos[v]++] = u;
         cols[highpos[u]++] = v;
     }
+    return PHEM_OK;
+}
+
+// Draws [first, first + count) of the same R-MAT stream as phem_gen_rmat,
+// unsorted: packed (lo << 32 | hi), self-loops dropped, draw order kept.  A
+// streaming consumer generates a huge graph batch by batch this way.
+phem_status phem_gen_rmat_range(uint32_t scale, uint64_t first, uint64_t count, double a, double b, double c,
+                                uint64_t seed, uint64_t *out, uint64_t *out_m)
+{
+    if (scale < 1 || scale > 31 || !out_m || a < 0 || b < 0 || c < 0 || a + b + c > 1.0)
+        return PHEM_ERR_INVALID;
+    const RmatDraw draw(scale, a, b, c, seed);
+    *out_m = emit_in_draw_order(count, out, [&](uint64_t i, uint64_t *val) {
+        uint32_t lo, hi;
+        if (!draw(first + i, &lo, &hi))
+            return false;
+        *val = ((uint64_t)lo << 32) | hi;
+        return true;
+    });
     return PHEM_OK;
 }
 

@@ -161,3 +161,29 @@ def test_stage_entry_points_and_reference_pipeline(ctx):
     ctx.cc_label(n, parent, label)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(label.cpu().numpy(), labels)
+
+
+def test_stream_unsorted_rmat_batches(ctx):
+    """SpanningTree over an unsorted R-MAT stream in ragged batches: labels
+    equal the oracle's, the forest reproduces them."""
+    import ctypes as C
+    import torch
+    scale, draws = 18, 32 << 18
+    out = np.empty(draws, np.uint64)
+    m = C.c_uint64()
+    _lib.check(_lib.lib().phem_gen_rmat_range(scale, 0, draws, 0.57, 0.19, 0.19, 28, out.ctypes.data, C.byref(m)),
+               "phem_gen_rmat_range")
+    pairs = out[: m.value]
+    n = 1 << scale
+    pinned = torch.from_numpy(pairs.view(np.int64)).pin_memory()
+    dev = torch.device("cuda", 0)
+    parent = torch.empty(n, dtype=torch.int32, device=dev)
+    label = torch.empty(n, dtype=torch.int32, device=dev)
+    forest = torch.empty(n, dtype=torch.int64, device=dev)
+    ctx.cc_stream(pinned.numpy().view(np.uint64), n, (1 << 20) + 12345, parent, label, forest)
+    ctx.cc_label(n, parent, label)
+    torch.cuda.synchronize()
+    want, _ = oracle.cc_solve(pairs, n)
+    got = label.cpu().numpy()
+    np.testing.assert_array_equal(got, want)
+    check_forest(pairs, n, got, forest.cpu().numpy().view(np.uint64))

@@ -127,3 +127,19 @@ def test_mixed_batch_layout_and_determinism():
     for i in range(a.num_graphs):
         e = a.graph_edges(i)
         assert np.all(e[:, :2] < int(g["num_vertices"][i])) and np.all(e[:, 0] < e[:, 1])
+
+
+def test_rmat_range_is_the_same_stream():
+    """Any split of the draw range gives, concatenated and sorted, the sorted
+    phem_gen_rmat output (same counter-based stream)."""
+    import ctypes as C
+    from phem_graph_b200._lib import lib
+    scale, draws = 12, 40000
+    parts = []
+    for first, cnt in ((0, 12345), (12345, 1), (12346, draws - 12346)):
+        out = np.empty(cnt, np.uint64)
+        m = C.c_uint64()
+        assert lib().phem_gen_rmat_range(scale, first, cnt, 0.57, 0.19, 0.19, 9, out.ctypes.data, C.byref(m)) == 0
+        parts.append(out[: m.value])
+    got = np.sort(np.concatenate(parts))
+    np.testing.assert_array_equal(got, gen.rmat(scale, draws, 9))
