@@ -116,6 +116,9 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
  *   "msf.next_batch"        rounds queued per later check                 [4]
  *   "msf.edge_items"        records per thread in the edge pass, 4 or 8   [8]
+ *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
+ *                           (a prefix of the list), compresses, then the
+ *                           rest; 0 unites all at once                     [2.0]
  *   "batch.block_size"      threads per CTA of the batched kernel,
  *                           256, 512 or 1024                               [512]
  *   "batch.items"           records per thread per step, 1, 2 or 4         [2]
@@ -417,6 +420,35 @@ phem_status phem_server_wait(phem_server *server, uint64_t ticket, uint32_t time
  * Returns the first submission error (results[i].status has each one). */
 phem_status phem_server_replay(phem_server *server, const phem_request *reqs, const uint64_t *arrival_ns,
                                uint32_t count, phem_request_result *results);
+
+/* ------------------------------------------------------------------ graph files */
+/* The reference drivers' input formats, read on the host (see io.cpp).
+ * Errors: PHEM_ERR_INVALID with phem_io_last_error() describing it. */
+
+/* MatrixMarket coordinate file as the MST driver reads it (getGraphInfo +
+ * mmapPopulateEdgeArray, MST/src/utils.cu:160-180, 896-1036): *n_out = rows,
+ * *m_out = nnz of the size line; out[i] = (min(u, v) - 1, max(u, v) - 1, w)
+ * of data line i, w read from the line or, with generate_weights, set to
+ * ((u - 1) * (v - 1) mod rows) + 1 in 32-bit arithmetic.  A missing or empty
+ * line gives {0, 0, 0}.  out == NULL queries the sizes. */
+phem_status phem_read_mtx(const char *path, int generate_weights, phem_edge *out, uint64_t capacity,
+                          uint32_t *n_out, uint64_t *m_out);
+
+/* ECL binary CSR as the CC driver reads it (readECLgraph, CC/graph.cu:90-121):
+ * int64 n, int64 nnz, int64 offsets[n + 1], int32 cols[nnz].  offsets or
+ * cols NULL queries the sizes. */
+phem_status phem_read_ecl(const char *path, int64_t *offsets, uint32_t *cols, uint64_t cols_capacity,
+                          uint32_t *n_out, uint64_t *nnz_out);
+
+/* The CC driver's input as packed pairs (u << 32 | v), u < v, in file order
+ * (undirected_graph, CC/graph.cu:13-196): ".edges", ".eg2" and ".txt" files
+ * are text edge lists ("n m" then m lines "u v"), any other name is ECL
+ * binary CSR converted in row-major order.  pairs NULL counts. */
+phem_status phem_read_graph_pairs(const char *path, uint64_t *pairs, uint64_t capacity, uint32_t *n_out,
+                                  uint64_t *m_out);
+
+/* Description of the last reader error of this thread. */
+const char *phem_io_last_error(void);
 
 /* --------------------------------------------------------- synthetic inputs (host) */
 /* Seeded generators for tests and benchmarks (no reference counterpart: the

@@ -286,3 +286,21 @@ def ref_serial_mst(E) -> np.ndarray:
     out = np.empty(max(len(E), 1), np.uint32)
     k = _ref_lib("libref_serial_mst.so").ref_serial_mst(E.reshape(-1), len(E), out)
     return np.sort(out[:k])
+
+
+def ref_mtx_read(path, generate_weights: bool = False):
+    """The MST driver's own MatrixMarket reader (getGraphInfo +
+    mmapPopulateEdgeArray, MST/src/utils.cu:160-180, 896-1036) on `path`:
+    ((m, 3) uint32 records, n), slots of missing lines left zero."""
+    L = _ref_lib("libref_mst.so")
+    L.ref_mtx_read.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint32),
+                               C.POINTER(C.c_uint64)]
+    L.ref_mtx_read.restype = C.c_int
+    p = str(path).encode()
+    n, m = C.c_uint32(), C.c_uint64()
+    if L.ref_mtx_read(p, int(generate_weights), None, 0, C.byref(n), C.byref(m)) != 0:
+        raise ValueError("reference reader failed")
+    out = np.zeros((max(m.value, 1), 3), np.uint32)
+    if L.ref_mtx_read(p, int(generate_weights), out.ctypes.data, m.value, C.byref(n), C.byref(m)) != 0:
+        raise ValueError("reference reader failed")
+    return out[: m.value], n.value

@@ -106,3 +106,36 @@ void ref_mst_ids(void *p, uint32_t *out)
 int32_t ref_mst_workers(void) { return (int32_t)parlay::num_workers(); }
 
 }  // extern "C"
+
+extern "C" {
+
+// The MST driver's MatrixMarket reader (getGraphInfo + mmapPopulateEdgeArray,
+// MST/src/utils.cu:160-180, 896-1036) on `path`: *n, *m from the size line;
+// uvw (3 * capacity uint32, zero-filled here as fresh pinned pages are) gets
+// the records.  Returns 0, or 1 when capacity < m.
+int ref_mtx_read(const char *path, int generate_weights, uint32_t *uvw, uint64_t capacity, uint32_t *n, uint64_t *m)
+{
+    std::ifstream file(path);
+    vertex num_nodes = 0;
+    large_vertex num_edges = 0;
+    {
+        QuietStdout quiet;
+        getGraphInfo(file, num_nodes, num_edges);
+    }
+    *n = num_nodes;
+    *m = num_edges;
+    if (!uvw)
+        return 0;
+    if (capacity < num_edges)
+        return 1;
+    std::vector<edge> e(num_edges ? num_edges : 1, edge{0, 0, 0});
+    {
+        QuietStdout quiet;
+        mmapPopulateEdgeArray(path, e.data(), (vertex)num_edges, num_nodes, generate_weights != 0);
+    }
+    memcpy(uvw, e.data(), sizeof(edge) * num_edges);
+    return 0;
+}
+
+}  // extern "C"
+

@@ -133,6 +133,11 @@ SIGNATURES = {
     "phem_csr_from_sorted_pairs": (C.c_int, [_VP, C.c_uint64, C.c_uint32, _VP, _VP]),
     "phem_gen_rmat_range": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double,
                                       C.c_uint64, _VP, C.POINTER(C.c_uint64)]),
+    "phem_read_mtx": (C.c_int, [C.c_char_p, C.c_int, _VP, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    "phem_read_ecl": (C.c_int, [C.c_char_p, _VP, _VP, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    "phem_read_graph_pairs": (C.c_int, [C.c_char_p, _VP, C.c_uint64, C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_uint64)]),
+    "phem_io_last_error": (C.c_char_p, []),
     "phem_gen_rgg": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, _VP, _VP, C.POINTER(C.c_uint64)]),
     "phem_batch_solve": (C.c_int, [_VP, _VP, C.c_uint32, _VP, C.c_uint64, C.c_uint32, _VP, _VP, _VP, _VP,
                                    C.POINTER(BatchStats)]),

@@ -406,6 +406,8 @@ phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double v
         ctx->tune_next_batch = (int)value;
     } else if (k == "msf.edge_items" && (value == 4 || value == 8)) {
         ctx->tune_edge_items = (int)value;
+    } else if (k == "cc.sample_per_vertex" && value >= 0.0 && value < 1e6) {
+        ctx->tune_cc_sample = value;
     } else if (k == "batch.block_size" && (value == 256 || value == 512 || value == 1024)) {
         ctx->tune_batch_block = (int)value;
     } else if (k == "batch.items" && (value == 1 || value == 2 || value == 4)) {
@@ -437,6 +439,8 @@ phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *
         *value = ctx->tune_next_batch;
     else if (k == "msf.edge_items")
         *value = ctx->tune_edge_items;
+    else if (k == "cc.sample_per_vertex")
+        *value = ctx->tune_cc_sample;
     else if (k == "batch.block_size")
         *value = ctx->tune_batch_block;
     else if (k == "batch.items")
@@ -517,7 +521,17 @@ phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, i
         int32_t *d_par = reinterpret_cast<int32_t *>(static_cast<char *>(ctx->ws) + base + o_par);
         PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), ctx->stream));
         PHEM_TRY(cc_launch_init(ctx, n, d_par, nullptr, d_for));
-        PHEM_TRY(cc_launch_unite(ctx, d_edges, m, n, d_par, d_for));
+        // a prefix sample of about tune_cc_sample edges per vertex builds the
+        // big components, a compress points every vertex at its root, and
+        // the remaining edges then mostly settle with two loads
+        int64_t s = (int64_t)(ctx->tune_cc_sample * (double)n) & ~int64_t(1);
+        if (s <= 0 || s >= m)
+            s = m;
+        PHEM_TRY(cc_launch_unite(ctx, d_edges, s, n, d_par, d_for));
+        if (s < m) {
+            PHEM_TRY(cc_launch_compress(ctx, n, d_par));
+            PHEM_TRY(cc_launch_unite(ctx, d_edges + s, m - s, n, d_par, d_for));
+        }
         PHEM_TRY(cc_launch_label(ctx, n, d_par, d_lab));
     }
     const float ms = timer.stop();

@@ -15,8 +15,9 @@
 //   hook      every component with an offer takes its minimum edge; a mutual
 //             pair keeps the lower root (new_grafting_edges,
 //             MST/src/kernels.cu:73-134); the edge is marked in a bitmap;
-//   compress  every vertex is jumped to its root (new_shortcutting_step,
-//             MST/src/kernels.cu:254-271) and best is reset;
+//   compress  every live root is jumped to its new root (new_shortcutting_step,
+//             MST/src/kernels.cu:254-271), best is reset and the roots that
+//             still hold edges form the next round's list;
 //   relabel   the survivor list is relabelled to roots; internal edges die
 //             (relabelling_step/filtering_step, MST/src/kernels.cu:273-321);
 //             the list is compacted in place when enough records died.
@@ -24,8 +25,10 @@
 // Keys are (w << 32 | id) for MSF graphs and id alone for CC graphs, so a CC
 // graph's forest is the canonical one (the MSF under edge index order) and
 // its labels are the minimum vertex id of each component.  The per-vertex
-// state (parent, root, best key: 16 bytes a vertex) lives in dynamic shared
-// memory when the graph fits, else in a global region of the graph's own.
+// state (best key, parent, scratch, live-root list: 20 bytes a vertex) lives
+// in dynamic shared memory when the graph fits, else in a global region of
+// the graph's own.  After the first round a round touches only the roots
+// still holding edges, so its vertex work shrinks with the components.
 //
 // Tuning: block size B and records per thread I are template parameters, the
 // compaction threshold is a run-time ratio; the autotuner in batch_api.cu
@@ -120,17 +123,38 @@ struct BatchSmem {
     uint32_t err;
 };
 
+// Root of x by path halving over the graph's parent array (shared or global
+// memory), bounded by n + 1 steps.  Concurrent halving writes point vertices
+// at ancestors, so walks that overlap them stay correct.
+__device__ __forceinline__ uint32_t g_find(uint32_t *parent, uint32_t x, uint32_t n, uint32_t *err)
+{
+    for (uint32_t steps = 0; steps <= n; steps++) {
+        const uint32_t p = *(volatile uint32_t *)(parent + x);
+        if (p == x)
+            return x;
+        const uint32_t gp = *(volatile uint32_t *)(parent + p);
+        if (gp == p)
+            return p;
+        parent[x] = gp;
+        x = gp;
+    }
+    atomicOr(err, kErrChase);
+    return x;
+}
+
 // One relabel/filter pass over the graph's edges.  FIRST reads the input
 // records (ids = positions) and always compacts into the survivor list;
 // later passes read the list and compact in place when `compact` is set
 // (writes never overtake reads: an iteration's survivors land below the end
-// of its own slots, and all its reads precede the scan barrier).  Returns the
-// survivor count; *len_out gets the new list length.
+// of its own slots, and all its reads precede the scan barrier).  `fresh`
+// lists were written by the previous pass, so their endpoints are roots the
+// last compress pointed straight at the current roots: one load relabels
+// them; older records walk with g_find.  Returns the survivor count;
+// *len_out gets the new list length.
 template <int B, int I, bool FIRST>
 __device__ uint32_t relabel_pass(const phem_edge *e0, const unsigned long long *p0, uint4 *wl, uint32_t len,
-                                 bool compact, uint32_t n,
-                                 uint32_t kind, const uint32_t *comp, unsigned long long *best,
-                                 BatchSmem<B> &sm, uint32_t *len_out)
+                                 bool compact, bool fresh, uint32_t n, uint32_t kind, uint32_t *parent,
+                                 unsigned long long *best, BatchSmem<B> &sm, uint32_t *len_out)
 {
     uint32_t out = 0, live = 0;
     int parity = 0;
@@ -154,11 +178,22 @@ __device__ uint32_t relabel_pass(const phem_edge *e0, const unsigned long long *
                     }
                 } else {
                     rec[j] = wl[i];
-                    rec[j].x = comp[rec[j].x];
-                    rec[j].y = comp[rec[j].y];
-                    keep[j] = rec[j].x != rec[j].y;
                 }
             }
+        }
+        if (!FIRST) {
+#pragma unroll
+            for (int j = 0; j < I; j++)
+                if (base + j * B + threadIdx.x < len) {
+                    if (fresh) {
+                        rec[j].x = *(volatile uint32_t *)(parent + rec[j].x);
+                        rec[j].y = *(volatile uint32_t *)(parent + rec[j].y);
+                    } else {
+                        rec[j].x = g_find(parent, rec[j].x, n, &sm.err);
+                        rec[j].y = g_find(parent, rec[j].y, n, &sm.err);
+                    }
+                    keep[j] = rec[j].x != rec[j].y;
+                }
         }
 #pragma unroll
         for (int j = 0; j < I; j++)
@@ -187,6 +222,14 @@ __device__ uint32_t relabel_pass(const phem_edge *e0, const unsigned long long *
     return live;
 }
 
+// Per-graph vertex state: best key (8 bytes), parent, aux (the chosen
+// edge's far root during a round, min-id labels at the end) and the list of
+// live roots (4 bytes each) -- 20 bytes a vertex.
+struct GraphState {
+    unsigned long long *best;
+    uint32_t *parent, *aux, *roots;
+};
+
 template <int B, int I>
 __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B> &sm, unsigned char *dyn)
 {
@@ -195,24 +238,34 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
     const unsigned long long *p0 = it.kind == kBatchPairs ? a.pairs + it.e_off : nullptr;
     uint4 *wl = a.wl + it.wl_off;
     uint32_t *bm = a.bitmap + it.bm_off;
-    const bool local = n <= a.smem_vertices;
-    uint32_t *parent = local ? reinterpret_cast<uint32_t *>(dyn) : a.g_parent + it.v_off;
-    uint32_t *comp = local ? reinterpret_cast<uint32_t *>(dyn) + a.smem_vertices : a.g_comp + it.v_off;
-    unsigned long long *best = local ? reinterpret_cast<unsigned long long *>(dyn + 8 * (size_t)a.smem_vertices)
-                                     : a.g_best + it.v_off;
+    GraphState g;
+    if (n <= a.smem_vertices) {
+        const size_t S = a.smem_vertices;
+        g.best = reinterpret_cast<unsigned long long *>(dyn);
+        g.parent = reinterpret_cast<uint32_t *>(dyn + 8 * S);
+        g.aux = reinterpret_cast<uint32_t *>(dyn + 12 * S);
+        g.roots = reinterpret_cast<uint32_t *>(dyn + 16 * S);
+    } else {
+        g.best = a.g_best + it.v_off;
+        g.parent = a.g_parent + it.v_off;
+        g.aux = a.g_aux + it.v_off;
+        g.roots = a.g_roots + it.v_off;
+    }
     const uint32_t nwords = (m + 31) / 32;
 
     for (uint32_t x = threadIdx.x; x < n; x += B) {
-        parent[x] = x;
-        comp[x] = x;
-        best[x] = kKeyInf;
+        g.parent[x] = x;
+        g.roots[x] = x;
+        g.best[x] = kKeyInf;
     }
     for (uint32_t w = threadIdx.x; w < nwords; w += B)
         bm[w] = 0;
     __syncthreads();
 
     uint32_t len = 0;
-    uint32_t live = relabel_pass<B, I, true>(e0, p0, wl, m, true, n, it.kind, comp, best, sm, &len);
+    uint32_t live = relabel_pass<B, I, true>(e0, p0, wl, m, true, true, n, it.kind, g.parent, g.best, sm, &len);
+    bool fresh = true;
+    uint32_t nroots = n;  // roots that may hold an offer
     uint32_t rounds = 0;
     while (live > 0) {
         if (++rounds > kBatchMaxRounds) {
@@ -221,53 +274,75 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
             break;
         }
         __syncthreads();  // offers complete
-        // hook: each component with an offer takes its minimum edge
-        for (uint32_t x = threadIdx.x; x < n; x += B) {
-            const unsigned long long k = best[x];
+        // A: the far root of each component's chosen edge, before any hook
+        for (uint32_t i = threadIdx.x; i < nroots; i += B) {
+            const uint32_t x = g.roots[i];
+            const unsigned long long k = g.best[x];
             if (k == kKeyInf)
                 continue;
-            const uint32_t id = (uint32_t)k;
             uint32_t eu, ev, ew;
-            load_edge(e0, p0, id, eu, ev, ew);
-            const uint32_t cu = comp[eu], cv = comp[ev];
-            const uint32_t other = cu == x ? cv : cu;
-            if (best[other] == k && x < other)
-                continue;  // mutual pair: the lower root stays a root
-            parent[x] = other;
+            load_edge(e0, p0, (uint32_t)k, eu, ev, ew);
+            const uint32_t ru = g_find(g.parent, eu, n, &sm.err), rv = g_find(g.parent, ev, n, &sm.err);
+            g.aux[x] = ru == x ? rv : ru;
+        }
+        __syncthreads();
+        // B: hook; a mutual pair keeps the lower root
+        for (uint32_t i = threadIdx.x; i < nroots; i += B) {
+            const uint32_t x = g.roots[i];
+            const unsigned long long k = g.best[x];
+            if (k == kKeyInf)
+                continue;
+            const uint32_t other = g.aux[x];
+            if (g.best[other] == k && x < other)
+                continue;
+            g.parent[x] = other;
+            const uint32_t id = (uint32_t)k;
             atomicOr(bm + (id >> 5), 1u << (id & 31));
         }
         __syncthreads();
-        // compress: every vertex to its root, best reset
-        for (uint32_t x = threadIdx.x; x < n; x += B) {
-            uint32_t r = x;
-            for (uint32_t steps = 0; steps <= n; steps++) {
-                const uint32_t p = *(volatile uint32_t *)(parent + r);
-                if (p == r)
-                    break;
-                r = p;
+        // C: point every listed root at its new root, reset best, and keep the
+        // roots that had an offer and are still roots (the others are done)
+        uint32_t kept = 0;
+        int parity = 0;
+        for (uint32_t i0 = 0; i0 < nroots; i0 += B) {
+            const uint32_t i = i0 + threadIdx.x;
+            bool keep = false;
+            uint32_t x = 0;
+            if (i < nroots) {
+                x = g.roots[i];
+                const bool had = g.best[x] != kKeyInf;
+                const uint32_t r = g_find(g.parent, x, n, &sm.err);
+                if (r != x)
+                    g.parent[x] = r;
+                g.best[x] = kKeyInf;
+                keep = had && r == x;
             }
-            if (*(volatile uint32_t *)(parent + r) != r)
-                atomicOr(&sm.err, kErrChase);
-            comp[x] = r;
-            if (parent[x] != r)
-                parent[x] = r;
-            best[x] = kKeyInf;
+            uint32_t total = 0;
+            const uint32_t pos = block_scan<B>(keep ? 1u : 0u, sm.scan, parity, &total);
+            parity ^= 1;
+            if (keep)
+                g.roots[kept + pos] = x;
+            kept += total;
         }
+        nroots = kept;
         __syncthreads();
         const bool compact = (float)live <= a.compact_ratio * (float)len;
-        live = relabel_pass<B, I, false>(e0, p0, wl, len, compact, n, it.kind, comp, best, sm, &len);
+        live = relabel_pass<B, I, false>(e0, p0, wl, len, compact, fresh, n, it.kind, g.parent, g.best, sm, &len);
+        fresh = compact;
     }
     __syncthreads();
 
-    // labels: minimum vertex id of each component (comp is final)
-    for (uint32_t x = threadIdx.x; x < n; x += B)
-        parent[x] = kNoVertex;
+    // labels: minimum vertex id of each component
+    for (uint32_t x = threadIdx.x; x < n; x += B) {
+        g.roots[x] = g_find(g.parent, x, n, &sm.err);
+        g.aux[x] = kNoVertex;
+    }
     __syncthreads();
     for (uint32_t x = threadIdx.x; x < n; x += B)
-        atomicMin(parent + comp[x], x);
+        atomicMin(g.aux + g.roots[x], x);
     __syncthreads();
     for (uint32_t x = threadIdx.x; x < n; x += B)
-        a.labels[it.v_off + x] = (int32_t)parent[comp[x]];
+        a.labels[it.v_off + x] = (int32_t)g.aux[g.roots[x]];
 
     // forest edges ascending by id, and the total weight
     uint32_t out = 0;
@@ -383,7 +458,7 @@ phem_status batch_launch_config(int device, int sm_count, int block, int items, 
     out->block = block;
     out->items = items;
     out->dyn_smem = dyn;
-    out->smem_vertices = (uint32_t)(dyn / 16);
+    out->smem_vertices = (uint32_t)(dyn / 20);
     out->grid = sm_count * occ;
     return PHEM_OK;
 }

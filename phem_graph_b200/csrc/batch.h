@@ -33,9 +33,10 @@ struct BatchArgs {
     const unsigned long long *pairs;  // kBatchPairs graphs' input (may be null otherwise)
     uint4 *wl;                   // sum of m records
     uint32_t *bitmap;            // sum of ceil(m / 32) words
-    uint32_t *g_parent;          // vertex state of graphs too large for shared memory
-    uint32_t *g_comp;
-    unsigned long long *g_best;
+    unsigned long long *g_best;  // vertex state of graphs too large for shared memory
+    uint32_t *g_parent;
+    uint32_t *g_aux;
+    uint32_t *g_roots;
     uint32_t *msf_ids;           // vertex-indexed: graph g's forest at [vertex_offset, + count)
     uint32_t *msf_count;         // per graph
     unsigned long long *msf_total;
@@ -59,7 +60,7 @@ struct BatchBuffers {
     uint32_t *num_graphs, *queue;
     phem_edge *edges;
     uint4 *wl;
-    uint32_t *bitmap, *g_parent, *g_comp;
+    uint32_t *bitmap, *g_parent, *g_aux, *g_roots;
     unsigned long long *g_best;
     uint32_t *msf_ids, *msf_count;
     unsigned long long *msf_total;

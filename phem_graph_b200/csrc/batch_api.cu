@@ -92,7 +92,7 @@ size_t batch_carve(uint32_t G, uint64_t E, uint64_t wl, uint64_t bm, uint32_t V,
     const size_t o_items = c.take<BatchItem>(g1), o_ng = c.take<uint32_t>(1), o_q = c.take<uint32_t>(1);
     const size_t o_e = edges_inline ? c.take<phem_edge>(E ? E : 1) : 0;
     const size_t o_wl = c.take<uint4>(wl ? wl : 1), o_bm = c.take<uint32_t>(bm ? bm : 1);
-    const size_t o_gp = c.take<uint32_t>(v1), o_gc = c.take<uint32_t>(v1);
+    const size_t o_gp = c.take<uint32_t>(v1), o_gc = c.take<uint32_t>(v1), o_gr = c.take<uint32_t>(v1);
     const size_t o_gb = c.take<unsigned long long>(v1);
     const size_t o_ids = c.take<uint32_t>(v1), o_cnt = c.take<uint32_t>(g1);
     const size_t o_tot = c.take<unsigned long long>(g1), o_lab = c.take<int32_t>(v1);
@@ -105,7 +105,8 @@ size_t batch_carve(uint32_t G, uint64_t E, uint64_t wl, uint64_t bm, uint32_t V,
         b->wl = reinterpret_cast<uint4 *>(base + o_wl);
         b->bitmap = reinterpret_cast<uint32_t *>(base + o_bm);
         b->g_parent = reinterpret_cast<uint32_t *>(base + o_gp);
-        b->g_comp = reinterpret_cast<uint32_t *>(base + o_gc);
+        b->g_aux = reinterpret_cast<uint32_t *>(base + o_gc);
+        b->g_roots = reinterpret_cast<uint32_t *>(base + o_gr);
         b->g_best = reinterpret_cast<unsigned long long *>(base + o_gb);
         b->msf_ids = reinterpret_cast<uint32_t *>(base + o_ids);
         b->msf_count = reinterpret_cast<uint32_t *>(base + o_cnt);
@@ -127,7 +128,8 @@ BatchArgs make_args(const BatchBuffers &b, const phem_edge *edges, float ratio)
     a.wl = b.wl;
     a.bitmap = b.bitmap;
     a.g_parent = b.g_parent;
-    a.g_comp = b.g_comp;
+    a.g_aux = b.g_aux;
+    a.g_roots = b.g_roots;
     a.g_best = b.g_best;
     a.msf_ids = b.msf_ids;
     a.msf_count = b.msf_count;

@@ -23,18 +23,33 @@
 namespace phem {
 namespace {
 
+// parent[i] through L1 (ld.global.ca).  Another SM's hook may not be seen
+// yet, but every value read is still an ancestor of i (a vertex's ancestors
+// only grow), so a walk on such values ends at an ancestor that may have
+// stopped being a root; the CAS that would hook it then fails, and the
+// retry reads through L2.  The gain: the few roots that most walks end at
+// (a giant component's) are served by each SM's L1 instead of one L2 slice.
+__device__ __forceinline__ int32_t ld_ca(const int32_t *p)
+{
+    int32_t v;
+    asm volatile("ld.global.ca.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
 // Root of x with path halving.  Writes only touch non-roots (a vertex that is
 // not a root never becomes one again), so they cannot race with the CAS that
 // hooks a root; each write points a vertex at one of its ancestors.  A path
-// has fewer than n + 1 vertices, so n + 1 steps bound the walk.
+// has fewer than n + 1 vertices, so n + 1 steps bound the walk.  CACHED walks
+// read through L1 (see ld_ca); the others read L2-coherently.
+template <bool CACHED>
 __device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x, int32_t n, uint32_t *err)
 {
     const uint32_t cap = (uint32_t)n + 1;
     for (uint32_t steps = 0; steps < cap; steps++) {
-        const int32_t p = __ldcg(parent + x);
+        const int32_t p = CACHED ? ld_ca(parent + x) : __ldcg(parent + x);
         if (p == x)
             return x;
-        const int32_t gp = __ldcg(parent + p);
+        const int32_t gp = CACHED ? ld_ca(parent + p) : __ldcg(parent + p);
         if (gp == p)
             return p;
         parent[x] = gp;
@@ -49,9 +64,19 @@ __device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x, int32_t n
 __device__ __forceinline__ bool uf_unite(int32_t *parent, unsigned long long *forest, unsigned long long e,
                                          int32_t u, int32_t v, int32_t n, uint32_t *err)
 {
+    {
+        // two independent loads settle most edges once parents point at roots
+        // (after a compress): equal parents mean one component
+        const int32_t pu = ld_ca(parent + u), pv = ld_ca(parent + v);
+        if (pu == pv)
+            return false;
+        u = pu;  // ancestors of the endpoints
+        v = pv;
+    }
     for (uint32_t retry = 0; retry < kUnionRetryCap; retry++) {
-        const int32_t ru = uf_find(parent, u, n, err);
-        const int32_t rv = uf_find(parent, v, n, err);
+        // first attempt through L1; after a failed CAS, coherent walks
+        const int32_t ru = retry == 0 ? uf_find<true>(parent, u, n, err) : uf_find<false>(parent, u, n, err);
+        const int32_t rv = retry == 0 ? uf_find<true>(parent, v, n, err) : uf_find<false>(parent, v, n, err);
         if (ru == rv)
             return false;
         if ((retry & 63) == 63 && (*(volatile uint32_t *)err & (kErrChase | kErrRetry)))
@@ -135,8 +160,20 @@ __global__ void __launch_bounds__(kBlock) cc_label_kernel(int32_t n, int32_t *pa
 {
     const int32_t stride = gridDim.x * blockDim.x;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const int32_t r = uf_find(parent, i, n, err);
+        const int32_t r = uf_find<false>(parent, i, n, err);
         label[i] = r;
+        if (parent[i] != r)
+            parent[i] = r;
+    }
+}
+
+// parent[i] = root(i) for every vertex (no labels): after it every later
+// union's first two loads already compare roots.
+__global__ void __launch_bounds__(kBlock) cc_compress_kernel(int32_t n, int32_t *parent, uint32_t *err)
+{
+    const int32_t stride = gridDim.x * blockDim.x;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int32_t r = uf_find<false>(parent, i, n, err);
         if (parent[i] != r)
             parent[i] = r;
     }
@@ -214,6 +251,14 @@ phem_status cc_launch_unite(phem_context *ctx, const uint64_t *edges, int64_t m,
     cc_unite_kernel<<<grid_for(ctx, (m + 1) / 2, 8), kBlock, 0, ctx->stream>>>(
         reinterpret_cast<const unsigned long long *>(edges), m, n, parent,
         reinterpret_cast<unsigned long long *>(forest), &ctx->ctl->err);
+    PHEM_CUDA_TRY(cudaGetLastError());
+    return PHEM_OK;
+}
+
+phem_status cc_launch_compress(phem_context *ctx, int32_t n, int32_t *parent)
+{
+    KernelScope k(ctx, kKCcLabel);
+    cc_compress_kernel<<<grid_for(ctx, n, 8), kBlock, 0, ctx->stream>>>(n, parent, &ctx->ctl->err);
     PHEM_CUDA_TRY(cudaGetLastError());
     return PHEM_OK;
 }

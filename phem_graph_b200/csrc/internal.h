@@ -54,6 +54,7 @@ struct phem_context {
     int tune_batch_block = 512;          // batched kernel: threads per CTA
     int tune_batch_items = 2;            // batched kernel: records per thread per step
     double tune_batch_compact = 0.5;     // batched kernel: compaction threshold
+    double tune_cc_sample = 2.0;         // CC: edges per vertex united before the first compress
     // launch accounting and optional per-kernel CUDA-event timing
     uint64_t launches[phem::kKernelCount] = {};
     double kernel_ms[phem::kKernelCount] = {};
@@ -248,6 +249,8 @@ phem_status cc_launch_init(phem_context *ctx, int32_t n, int32_t *parent, int32_
 phem_status cc_launch_unite(phem_context *ctx, const uint64_t *edges, int64_t m, int32_t n, int32_t *parent,
                             uint64_t *forest);
 phem_status cc_launch_label(phem_context *ctx, int32_t n, int32_t *parent, int32_t *label);
+// parent[i] = root(i) for all i.
+phem_status cc_launch_compress(phem_context *ctx, int32_t n, int32_t *parent);
 phem_status cc_launch_merge(phem_context *ctx, const uint64_t *fa, const uint64_t *fb, int32_t n, int32_t *parent,
                             uint64_t *forest_out);
 // min-id labels from an arbitrary-root parent array (canonical forest path)

@@ -342,9 +342,9 @@ phem_status phem_server_create(int device, const phem_server_config *cfg, phem_s
     s->device = device;
     s->cfg = *cfg;
     // half of the budget for the batch slots: per edge 12 B input + 8 B pairs
-    // + 16 B list + bitmap; per vertex 16 B state + 8 B outputs, sized with
+    // + 16 B list + bitmap; per vertex 20 B state + 8 B outputs, sized with
     // one vertex per edge
-    const uint64_t per_edge = 12 + 8 + 16 + 1 + 24;
+    const uint64_t per_edge = 12 + 8 + 16 + 1 + 28;
     uint64_t e = cfg->memory_budget / 2 / cfg->slots / per_edge;
     e = std::min<uint64_t>(e, 1ull << 26);
     s->slot_edges = std::max<uint64_t>(e, cfg->large_edges);

@@ -187,3 +187,37 @@ def test_stream_unsorted_rmat_batches(ctx):
     got = label.cpu().numpy()
     np.testing.assert_array_equal(got, want)
     check_forest(pairs, n, got, forest.cpu().numpy().view(np.uint64))
+
+
+@pytest.mark.parametrize("sample", [0.0, 0.5, 2.0, 1000.0])
+def test_sample_schedule_same_labels(ctx, sample):
+    """The prefix-sample / compress / rest schedule gives the same labels and
+    a valid forest for any sample size."""
+    g = gen.er_graph(1 << 16, 1 << 19, 9)
+    want, _ = oracle.cc_solve(g.pairs, g.n)
+    saved = ctx.get_tuning("cc.sample_per_vertex")
+    try:
+        ctx.set_tuning("cc.sample_per_vertex", sample)
+        r = ctx.cc_solve(g.pairs, g.n)
+    finally:
+        ctx.set_tuning("cc.sample_per_vertex", saved)
+    np.testing.assert_array_equal(r.labels, want)
+    check_forest(g.pairs, g.n, r.labels, r.forest)
+
+
+def test_solves_from_reference_file_formats(ctx, tmp_path):
+    """Inputs read from the reference drivers' file formats solve to the
+    oracle's results (ECL binary CSR for CC, MatrixMarket for MSF)."""
+    from phem_graph_b200 import io
+    g = gen.rmat_graph(12, 8, seed=6)
+    off, cols = gen.csr_from_pairs(g.pairs, g.n)
+    io.write_ecl(tmp_path / "g.egr", off, cols)
+    pairs, n = io.read_graph_pairs(tmp_path / "g.egr")
+    want, _ = oracle.cc_solve(pairs, n)
+    np.testing.assert_array_equal(ctx.cc_solve(pairs, n).labels, want)
+    io.write_mtx(tmp_path / "g.mtx", g.msf_edges(), g.n)
+    e, n = io.read_mtx(tmp_path / "g.mtx")
+    flags, cnt, tot = oracle.msf_kruskal(e, n)
+    r = ctx.msf_solve(e, n)
+    assert (r.count, r.total) == (cnt, tot)
+    np.testing.assert_array_equal(r.edges, e[flags])
