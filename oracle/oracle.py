@@ -32,6 +32,9 @@ def build(reference: str | None = None) -> None:
     ref = reference or os.environ.get("PHEM_REFERENCE", "/root/reference")
     if Path(ref, "CC", "host_spanning_tree.cu").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), f"REF={ref}", "ref"], check=True)
+        if (HERE.parent / "phem_graph_b200" / "libphem.so").exists():
+            # the reference drivers linked with the compat layer (checks of the boundary)
+            subprocess.run(["make", "-s", "-C", str(HERE), f"REF={ref}", "compat"], check=True)
 
 
 def lib() -> C.CDLL:
