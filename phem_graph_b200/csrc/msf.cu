@@ -108,6 +108,56 @@ __device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, 
     }
 }
 
+// Per-CTA shared-memory pre-reduction of offers for rounds with few live
+// components: most survivors of such rounds offer to a handful of hub
+// components, and the same best[] words then serialise on one L2 slice.
+// A root owns a slot (t mod kOfferSlots) once it claims it; offers to owned
+// slots are shared-memory atomicMin, the rest go to best[] directly, and the
+// slots are flushed to best[] when the CTA's tiles are done.
+constexpr int kOfferSlots = 1024;
+constexpr uint32_t kNoTag = 0xffffffffu;
+constexpr unsigned long long kCacheMaxComponents = 1ull << 18;
+
+// Slot of t, claiming it when free; -1 when another root holds it.
+__device__ __forceinline__ int offer_slot(uint32_t *tags, uint32_t t)
+{
+    const int slot = (int)(t & (kOfferSlots - 1));
+    uint32_t tag = *(volatile uint32_t *)(tags + slot);
+    if (tag == kNoTag)
+        tag = atomicCAS(tags + slot, kNoTag, t);
+    return (tag == kNoTag || tag == t) ? slot : -1;
+}
+
+// offer_row with the shared-memory slots: `slot` >= 0 sends the offer there.
+__device__ __forceinline__ void offer_row_cached(unsigned long long *best, unsigned long long *keys, uint32_t t,
+                                                 int slot, unsigned long long key, bool live,
+                                                 unsigned long long guard)
+{
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (!act)
+        return;
+    const int leader = __ffs(act) - 1;
+    const uint32_t t0 = __shfl_sync(0xffffffffu, t, leader);
+    if (__all_sync(0xffffffffu, !live || t == t0)) {
+        const uint32_t hi = live ? (uint32_t)(key >> 32) : 0xffffffffu;
+        const uint32_t lo = live ? (uint32_t)key : 0xffffffffu;
+        const uint32_t mhi = __reduce_min_sync(0xffffffffu, hi);
+        const uint32_t mlo = __reduce_min_sync(0xffffffffu, hi == mhi ? lo : 0xffffffffu);
+        const unsigned long long km = ((unsigned long long)mhi << 32) | mlo;
+        if ((int)lane_id() == leader) {
+            if (slot >= 0)
+                atomicMin(keys + slot, km);
+            else if (km < guard)
+                atomicMin(best + t0, km);
+        }
+    } else if (live) {
+        if (slot >= 0)
+            atomicMin(keys + slot, key);
+        else if (key < guard)
+            atomicMin(best + t, key);
+    }
+}
+
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
 {
 #pragma unroll
@@ -253,11 +303,20 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     __shared__ uint32_t s_cnt[kCnt];
     __shared__ unsigned long long s_base, s_base2;
     __shared__ uint32_t s_split, s_total;
+    __shared__ uint32_t s_tag[kOfferSlots];
+    __shared__ unsigned long long s_key[kOfferSlots];
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const uint32_t src = *(volatile uint32_t *)&ctl->src;
+    // list rounds with few components (those that chose an edge last round)
+    const bool cached = src == kSrcList && r > 0 && ctl->n_r[r - 1] <= kCacheMaxComponents;
+    if (cached)
+        for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
+            s_tag[i] = kNoTag;
+            s_key[i] = kKeyNone;
+        }
     const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
     const bool from_e0 = src != kSrcList;
     const uint64_t count = from_e0 ? a.m : ctl->wl_len[r - 1];
@@ -449,27 +508,47 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             bool on[4];
             unsigned long long key[4], ga[4], gb[4];
 #pragma unroll
+            int sa[4], sb[4];
+#pragma unroll
             for (int q = 0; q < 4; q++) {
                 const uint32_t i = i0 + q * kBlock + threadIdx.x;
                 on[q] = i < total;
                 rec[q] = on[q] ? staging[i] : make_uint4(0, 0, 0, 0);
                 key[q] = ((unsigned long long)rec[q].z << 32) | rec[q].w;
-                ga[q] = on[q] ? __ldcg(a.best + rec[q].x) : 0ull;
-                gb[q] = on[q] ? __ldcg(a.best + rec[q].y) : 0ull;
+                sa[q] = cached && on[q] ? offer_slot(s_tag, rec[q].x) : -1;
+                sb[q] = cached && on[q] ? offer_slot(s_tag, rec[q].y) : -1;
+                ga[q] = on[q] && sa[q] < 0 ? __ldcg(a.best + rec[q].x) : 0ull;
+                gb[q] = on[q] && sb[q] < 0 ? __ldcg(a.best + rec[q].y) : 0ull;
             }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const uint32_t i = i0 + q * kBlock + threadIdx.x;
                 if (on[q])
                     out[i < split ? base + i : base2 + (i - split)] = rec[q];
-                offer_row(a.best, rec[q].x, key[q], on[q], ga[q]);
-                offer_row(a.best, rec[q].y, key[q], on[q], gb[q]);
+                if (cached) {
+                    offer_row_cached(a.best, s_key, rec[q].x, sa[q], key[q], on[q], ga[q]);
+                    offer_row_cached(a.best, s_key, rec[q].y, sb[q], key[q], on[q], gb[q]);
+                } else {
+                    offer_row(a.best, rec[q].x, key[q], on[q], ga[q]);
+                    offer_row(a.best, rec[q].y, key[q], on[q], gb[q]);
+                }
             }
         }
         // this thread's staging writes and reads of the stage come before the
         // bulk copy that will refill it
         fence_proxy_async_smem();
         __syncthreads();  // staging, s_cnt and the bases are free again
+    }
+    if (cached) {  // flush the shared-memory slots to best[]
+        __syncthreads();
+        for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
+            const uint32_t tag = s_tag[i];
+            if (tag != kNoTag) {
+                const unsigned long long k = s_key[i];
+                if (k < __ldcg(a.best + tag))
+                    atomicMin(a.best + tag, k);
+            }
+        }
     }
     // pad the last chunk's unused tail with dead records and publish this
     // CTA's exact survivor count
