@@ -118,7 +118,7 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.edge_items"        records per thread in the edge pass, 4 or 8   [8]
  *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
  *                           (a prefix of the list), compresses, then the
- *                           rest; 0 unites all at once                     [2.0]
+ *                           rest; 0 unites all at once                     [0]
  *   "batch.block_size"      threads per CTA of the batched kernel,
  *                           256, 512 or 1024                               [512]
  *   "batch.items"           records per thread per step, 1, 2 or 4         [2]

@@ -54,7 +54,7 @@ struct phem_context {
     int tune_batch_block = 512;          // batched kernel: threads per CTA
     int tune_batch_items = 2;            // batched kernel: records per thread per step
     double tune_batch_compact = 0.5;     // batched kernel: compaction threshold
-    double tune_cc_sample = 2.0;         // CC: edges per vertex united before the first compress
+    double tune_cc_sample = 0.0;         // CC: edges per vertex united before a compress (0: one pass)
     // launch accounting and optional per-kernel CUDA-event timing
     uint64_t launches[phem::kKernelCount] = {};
     double kernel_ms[phem::kKernelCount] = {};

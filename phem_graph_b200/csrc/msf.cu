@@ -113,8 +113,12 @@ __device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, 
 // components, and the same best[] words then serialise on one L2 slice.
 // A root owns a slot (t mod kOfferSlots) once it claims it; offers to owned
 // slots are shared-memory atomicMin, the rest go to best[] directly, and the
-// slots are flushed to best[] when the CTA's tiles are done.
-constexpr int kOfferSlots = 1024;
+// slots are flushed to best[] when the CTA's tiles are done.  The slots live
+// in the last row of the three stage buffers, which list rounds leave free
+// (their tiles are one row shorter): more static shared memory would push
+// two CTAs per SM past a carveout step and halve the L1 the heavy pass's
+// relabel gathers rely on.
+constexpr int kOfferSlots = 1024;  // tags: 4 KB in stage 0; keys: 512 in stage 1, 512 in stage 2
 constexpr uint32_t kNoTag = 0xffffffffu;
 constexpr unsigned long long kCacheMaxComponents = 1ull << 18;
 
@@ -128,10 +132,10 @@ __device__ __forceinline__ int offer_slot(uint32_t *tags, uint32_t t)
     return (tag == kNoTag || tag == t) ? slot : -1;
 }
 
-// offer_row with the shared-memory slots: `slot` >= 0 sends the offer there.
-__device__ __forceinline__ void offer_row_cached(unsigned long long *best, unsigned long long *keys, uint32_t t,
-                                                 int slot, unsigned long long key, bool live,
-                                                 unsigned long long guard)
+// offer_row with the shared-memory slots: a non-null `kp` (the slot's key)
+// takes the offer there.
+__device__ __forceinline__ void offer_row_cached(unsigned long long *best, unsigned long long *kp, uint32_t t,
+                                                 unsigned long long key, bool live, unsigned long long guard)
 {
     const unsigned act = __ballot_sync(0xffffffffu, live);
     if (!act)
@@ -145,14 +149,14 @@ __device__ __forceinline__ void offer_row_cached(unsigned long long *best, unsig
         const uint32_t mlo = __reduce_min_sync(0xffffffffu, hi == mhi ? lo : 0xffffffffu);
         const unsigned long long km = ((unsigned long long)mhi << 32) | mlo;
         if ((int)lane_id() == leader) {
-            if (slot >= 0)
-                atomicMin(keys + slot, km);
+            if (kp)
+                atomicMin(kp, km);
             else if (km < guard)
                 atomicMin(best + t0, km);
         }
     } else if (live) {
-        if (slot >= 0)
-            atomicMin(keys + slot, key);
+        if (kp)
+            atomicMin(kp, key);
         else if (key < guard)
             atomicMin(best + t, key);
     }
@@ -296,26 +300,33 @@ __host__ __device__ constexpr size_t pipe_smem()
 template <int KIND, int ITEMS>
 __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
 {
-    constexpr int kTileRecs = kBlock * ITEMS;
     constexpr int kCnt = ITEMS * kWarps;  // row/warp counts per tile
     extern __shared__ __align__(128) unsigned char stage_mem[];
     __shared__ uint64_t s_bar[kStages];
     __shared__ uint32_t s_cnt[kCnt];
     __shared__ unsigned long long s_base, s_base2;
     __shared__ uint32_t s_split, s_total;
-    __shared__ uint32_t s_tag[kOfferSlots];
-    __shared__ unsigned long long s_key[kOfferSlots];
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const uint32_t src = *(volatile uint32_t *)&ctl->src;
+    // list rounds read tiles one row short, which frees the last row of every
+    // stage for the offer slots
+    const int rows = src == kSrcList ? ITEMS - 1 : ITEMS;
+    const uint32_t tile_recs = (uint32_t)rows * kBlock;
+    constexpr size_t kFreeRow = (size_t)(ITEMS - 1) * kBlock * 16;
+    uint32_t *s_tag = reinterpret_cast<uint32_t *>(stage_mem + kFreeRow);
+    unsigned long long *s_key0 = reinterpret_cast<unsigned long long *>(stage_mem + stage_bytes<ITEMS>() + kFreeRow);
+    unsigned long long *s_key1 =
+        reinterpret_cast<unsigned long long *>(stage_mem + 2 * stage_bytes<ITEMS>() + kFreeRow);
+    auto slot_key = [&](int i) { return i < kOfferSlots / 2 ? s_key0 + i : s_key1 + (i - kOfferSlots / 2); };
     // list rounds with few components (those that chose an edge last round)
     const bool cached = src == kSrcList && r > 0 && ctl->n_r[r - 1] <= kCacheMaxComponents;
     if (cached)
         for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
             s_tag[i] = kNoTag;
-            s_key[i] = kKeyNone;
+            *slot_key(i) = kKeyNone;
         }
     const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
     const bool from_e0 = src != kSrcList;
@@ -323,10 +334,10 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
     uint4 *out = (r & 1) ? a.wl1 : a.wl0;       // WL[r & 1]
     const uint32_t rec_bytes = from_e0 ? (KIND == kKindMsf ? 12u : 8u) : 16u;
-    const uint32_t tile_bytes = kTileRecs * rec_bytes;
+    const uint32_t tile_bytes = tile_recs * rec_bytes;
     const char *src_base = from_e0 ? static_cast<const char *>(a.e0) : reinterpret_cast<const char *>(in);
-    const uint64_t ntiles = (count + kTileRecs - 1) / kTileRecs;
-    const uint64_t full_tiles = count / kTileRecs;  // the partial last tile is read directly
+    const uint64_t ntiles = (count + tile_recs - 1) / tile_recs;
+    const uint64_t full_tiles = count / tile_recs;  // the partial last tile is read directly
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     // Output space is reserved in chunks of up to kChunk records per CTA (one
     // atomicAdd per chunk, not per tile); a tile that does not fit finishes the
@@ -362,14 +373,14 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         if (__syncthreads_or(!ok))
             break;  // a bulk copy never completed; the status bit is set
         unsigned char *stage = stage_mem + s * stage_bytes<ITEMS>();
-        const uint64_t tbase = t * kTileRecs;
+        const uint64_t tbase = t * tile_recs;
         uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
         bool keep[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; j++) {
             const uint32_t idx = j * kBlock + threadIdx.x;
             const uint64_t gi = tbase + idx;
-            const bool inb = gi < count;
+            const bool inb = j < rows && gi < count;
             if (from_e0) {
                 uint32_t u = 0, v = 0, ww = 0;
                 if (KIND == kKindMsf) {
@@ -477,7 +488,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                     s_split = (uint32_t)chunk_left;
                     const unsigned long long rest = total - chunk_left;
                     const uint64_t tiles_left = (ntiles - 1 - t) / gridDim.x + 1;
-                    const unsigned long long cap = tiles_left * kTileRecs;
+                    const unsigned long long cap = tiles_left * tile_recs;
                     const unsigned long long want = cap < kChunk ? cap : kChunk;
                     const unsigned long long size = want > rest ? want : rest;
                     const unsigned long long fresh = atomicAdd(&ctl->wl_len[r], size);
@@ -508,17 +519,19 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             bool on[4];
             unsigned long long key[4], ga[4], gb[4];
 #pragma unroll
-            int sa[4], sb[4];
+            unsigned long long *ka[4], *kb[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const uint32_t i = i0 + q * kBlock + threadIdx.x;
                 on[q] = i < total;
                 rec[q] = on[q] ? staging[i] : make_uint4(0, 0, 0, 0);
                 key[q] = ((unsigned long long)rec[q].z << 32) | rec[q].w;
-                sa[q] = cached && on[q] ? offer_slot(s_tag, rec[q].x) : -1;
-                sb[q] = cached && on[q] ? offer_slot(s_tag, rec[q].y) : -1;
-                ga[q] = on[q] && sa[q] < 0 ? __ldcg(a.best + rec[q].x) : 0ull;
-                gb[q] = on[q] && sb[q] < 0 ? __ldcg(a.best + rec[q].y) : 0ull;
+                const int sa = cached && on[q] ? offer_slot(s_tag, rec[q].x) : -1;
+                const int sb = cached && on[q] ? offer_slot(s_tag, rec[q].y) : -1;
+                ka[q] = sa >= 0 ? slot_key(sa) : nullptr;
+                kb[q] = sb >= 0 ? slot_key(sb) : nullptr;
+                ga[q] = on[q] && !ka[q] ? __ldcg(a.best + rec[q].x) : 0ull;
+                gb[q] = on[q] && !kb[q] ? __ldcg(a.best + rec[q].y) : 0ull;
             }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -526,8 +539,8 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
                 if (on[q])
                     out[i < split ? base + i : base2 + (i - split)] = rec[q];
                 if (cached) {
-                    offer_row_cached(a.best, s_key, rec[q].x, sa[q], key[q], on[q], ga[q]);
-                    offer_row_cached(a.best, s_key, rec[q].y, sb[q], key[q], on[q], gb[q]);
+                    offer_row_cached(a.best, ka[q], rec[q].x, key[q], on[q], ga[q]);
+                    offer_row_cached(a.best, kb[q], rec[q].y, key[q], on[q], gb[q]);
                 } else {
                     offer_row(a.best, rec[q].x, key[q], on[q], ga[q]);
                     offer_row(a.best, rec[q].y, key[q], on[q], gb[q]);
@@ -544,7 +557,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
         for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
             const uint32_t tag = s_tag[i];
             if (tag != kNoTag) {
-                const unsigned long long k = s_key[i];
+                const unsigned long long k = *slot_key(i);
                 if (k < __ldcg(a.best + tag))
                     atomicMin(a.best + tag, k);
             }
