@@ -329,6 +329,8 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             *slot_key(i) = kKeyNone;
         }
     const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
+    const uint32_t thr_hi = (uint32_t)(thr >> 32), thr_lo = (uint32_t)thr;
+    const bool light_round = src == kSrcLight;
     const bool from_e0 = src != kSrcList;
     const uint64_t count = from_e0 ? a.m : ctl->wl_len[r - 1];
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
@@ -374,47 +376,49 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             break;  // a bulk copy never completed; the status bit is set
         unsigned char *stage = stage_mem + s * stage_bytes<ITEMS>();
         const uint64_t tbase = t * tile_recs;
+        // per-record work in 32-bit arithmetic: edge ids are below 2^32
+        const uint64_t left64 = count - tbase;
+        const uint32_t rem = left64 < tile_recs ? (uint32_t)left64 : tile_recs;  // also excludes the free row
+        const uint32_t id0 = (uint32_t)tbase;
         uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
         bool keep[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; j++) {
             const uint32_t idx = j * kBlock + threadIdx.x;
-            const uint64_t gi = tbase + idx;
-            const bool inb = j < rows && gi < count;
+            const bool inb = idx < rem;
+            id[j] = id0 + idx;
             if (from_e0) {
                 uint32_t u = 0, v = 0, ww = 0;
-                if (KIND == kKindMsf) {
-                    const uint32_t *p = bulk ? reinterpret_cast<const uint32_t *>(stage) + 3 * idx
-                                             : static_cast<const uint32_t *>(a.e0) + 3 * gi;
-                    if (inb) {
+                if (inb) {
+                    if (KIND == kKindMsf) {
+                        const uint32_t *p = bulk ? reinterpret_cast<const uint32_t *>(stage) + 3 * idx
+                                                 : static_cast<const uint32_t *>(a.e0) + 3 * (tbase + idx);
                         u = p[0];
                         v = p[1];
                         ww = p[2];
+                    } else {
+                        const unsigned long long e = bulk
+                                                         ? reinterpret_cast<const unsigned long long *>(stage)[idx]
+                                                         : static_cast<const unsigned long long *>(a.e0)[tbase + idx];
+                        u = (uint32_t)(e >> 32);
+                        v = (uint32_t)e;
                     }
-                } else {
-                    const unsigned long long *p = bulk
-                                                      ? reinterpret_cast<const unsigned long long *>(stage) + idx
-                                                      : static_cast<const unsigned long long *>(a.e0) + gi;
-                    const unsigned long long e = inb ? *p : 0ull;
-                    u = (uint32_t)(e >> 32);
-                    v = (uint32_t)e;
                 }
-                bool ok_e = inb && e0_live<KIND>(u, v);
-                if (ok_e && (u >= a.n || v >= a.n)) {
-                    if (src == kSrcLight)
-                        set_err(&ctl->err, kErrRange);
-                    ok_e = false;
-                }
-                const bool light = e0_key<KIND>(ww, gi) < thr;
-                keep[j] = ok_e && (src == kSrcLight ? light : !light);
+                const bool live_e = inb && e0_live<KIND>(u, v);
+                const bool bad = live_e && max(u, v) >= a.n;
+                if (bad && light_round)
+                    set_err(&ctl->err, kErrRange);
+                // e0_key(w, id) < thr, compared as (high word, low word)
+                const bool light = KIND == kKindMsf ? (ww < thr_hi || (ww == thr_hi && id[j] < thr_lo))
+                                                    : (thr_hi != 0 || id[j] < thr_lo);
+                keep[j] = live_e && !bad && (light_round ? light : !light);
                 ra[j] = u;
                 rb[j] = v;
                 w[j] = ww;
-                id[j] = (uint32_t)gi;
             } else {
                 uint4 rec = make_uint4(0, 0, 0, 0);
                 if (inb)
-                    rec = bulk ? reinterpret_cast<const uint4 *>(stage)[idx] : __ldcs(in + gi);
+                    rec = bulk ? reinterpret_cast<const uint4 *>(stage)[idx] : __ldcs(in + (tbase + idx));
                 keep[j] = inb;
                 ra[j] = rec.x;
                 rb[j] = rec.y;
