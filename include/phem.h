@@ -111,7 +111,7 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
 
 /* Tuning knobs (defaults suit B200; the autotuner may change them):
  *   "msf.light_per_vertex"  light edges per vertex taken by the MSF filter
- *                           before the heavy pass; 0 disables the filter   [1.0]
+ *                           before the heavy pass; 0 disables the filter   [0.5]
  *   "msf.filter_min_ratio"  filter only when m >= ratio * light edges      [2.0]
  *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
  *   "msf.next_batch"        rounds queued per later check                 [4]

@@ -47,7 +47,7 @@ struct phem_context {
     int gather_blocks = 0;
     int tune_edge_items = 8;             // records per thread in the MSF edge pass (4 or 8)
     // tuning knobs (phem_context_set_tuning)
-    double tune_light_per_vertex = 1.0;  // light edges per vertex in the MSF filter (0: no filter)
+    double tune_light_per_vertex = 0.5;  // light edges per vertex in the MSF filter (0: no filter)
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
     int tune_first_batch = 8;            // Boruvka rounds queued before the first host check
     int tune_next_batch = 4;             // rounds queued per later check

@@ -66,11 +66,12 @@ def test_unfiltered_rounds_equal_boruvka_restatement(ctx, scale, ef):
     g = gen.rmat_graph(scale, ef, seed=scale)
     E = g.msf_edges()
     _, _, _, m_r, n_r = oracle.msf_boruvka(E, g.n)
+    saved = ctx.get_tuning("msf.light_per_vertex")
     ctx.set_tuning("msf.light_per_vertex", 0)
     try:
         r = ctx.msf_solve(E, g.n)
     finally:
-        ctx.set_tuning("msf.light_per_vertex", 1.0)
+        ctx.set_tuning("msf.light_per_vertex", saved)
     assert r.m_r == [int(x) for x in m_r] + [0]
     assert r.n_r == [int(x) for x in n_r] + [0]
 
