@@ -652,6 +652,8 @@ constexpr int kVItems = 4;  // candidates per thread per iteration of the vertex
 // block-iteration) and best is reset.  In the round where the light phase runs
 // dry every vertex is compressed to its root instead, so the heavy pass
 // relabels original endpoints in one hop.
+__device__ void advance_round(Ctl *ctl);
+
 __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
 {
     __shared__ uint32_t s_warp[kWarps];
@@ -729,12 +731,23 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
         }
         __syncthreads();  // s_warp / s_base reused next iteration
     }
+    // the last block to finish decides the next round (no separate launch)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctl->misc[6], 1ull) == gridDim.x - 1) {
+            __threadfence();
+            ctl->misc[6] = 0;
+            advance_round(ctl);
+        }
+    }
 }
 
 // Ends a round.  Live edges left -> another round on the survivor list.  No
 // light edge left -> switch to the heavy pass (if there is a threshold).  No
 // heavy edge left -> done.
-__global__ void advance_kernel(Ctl *ctl)
+// Decides the next round from this round's counters (one thread).
+__device__ void advance_round(Ctl *ctl)
 {
     if (!ctl->go)
         return;
@@ -761,10 +774,15 @@ __global__ void advance_kernel(Ctl *ctl)
     ctl->go = again ? 1u : 0u;
 }
 
+
+
 // Ordered gather: MSF records ascending by id from the bitmap, plus count and
 // uint64 total weight.
+constexpr uint32_t kGatherIds = 4096;  // ids a tile stages in shared memory (denser tiles use the direct path)
+
 __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *out)
 {
+    __shared__ uint32_t s_ids[kGatherIds];
     __shared__ uint32_t s_tile, s_base;
     __shared__ uint32_t s_warp[kWarps + 1];
     __shared__ unsigned long long s_red[kWarps];
@@ -798,24 +816,64 @@ __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *
                     ctl->msf_count = (unsigned long long)ex + total;
             }
         }
-        __syncthreads();
-        uint32_t pos = s_base + off;
         unsigned long long wsum = 0;
+        if (total <= kGatherIds) {
+            // the tile's ids go to shared memory in order, then every thread
+            // gathers independent records (coalesced writes, loads in flight)
+            uint32_t pos = off;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            uint32_t b = bits[j];
-            while (b) {
-                const int k = __ffs(b) - 1;
-                b &= b - 1;
-                const uint64_t id = (wbase + j) * 32 + k;
-                phem_edge e;
-                e.u = __ldg(E + id * 3);
-                e.v = __ldg(E + id * 3 + 1);
-                e.w = __ldg(E + id * 3 + 2);
-                if (out)
-                    out[pos] = e;
-                pos++;
-                wsum += e.w;
+            for (int j = 0; j < 4; j++) {
+                uint32_t b = bits[j];
+                while (b) {
+                    const int k = __ffs(b) - 1;
+                    b &= b - 1;
+                    s_ids[pos++] = (uint32_t)((wbase + j) * 32 + k);
+                }
+            }
+            __syncthreads();
+            const uint32_t base = s_base;
+            for (uint32_t i0 = 0; i0 < total; i0 += kBlock * 4) {
+                phem_edge e[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const uint32_t i = i0 + q * kBlock + threadIdx.x;
+                    e[q] = phem_edge{0, 0, 0};
+                    if (i < total) {
+                        const uint64_t id = s_ids[i];
+                        e[q].u = __ldg(E + id * 3);
+                        e[q].v = __ldg(E + id * 3 + 1);
+                        e[q].w = __ldg(E + id * 3 + 2);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const uint32_t i = i0 + q * kBlock + threadIdx.x;
+                    if (i < total) {
+                        if (out)
+                            out[base + i] = e[q];
+                        wsum += e[q].w;
+                    }
+                }
+            }
+        } else {
+            __syncthreads();
+            uint32_t pos = s_base + off;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                uint32_t b = bits[j];
+                while (b) {
+                    const int k = __ffs(b) - 1;
+                    b &= b - 1;
+                    const uint64_t id = (wbase + j) * 32 + k;
+                    phem_edge e;
+                    e.u = __ldg(E + id * 3);
+                    e.v = __ldg(E + id * 3 + 1);
+                    e.w = __ldg(E + id * 3 + 2);
+                    if (out)
+                        out[pos] = e;
+                    pos++;
+                    wsum += e.w;
+                }
             }
         }
         const unsigned long long bs = block_sum_u64(wsum, s_red);
@@ -870,10 +928,6 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
     {
         KernelScope k(ctx, kKCompress);
         compress_kernel<<<vb, kBlock, 0, ctx->stream>>>(a);
-    }
-    {
-        KernelScope k(ctx, kKAdvance);
-        advance_kernel<<<1, 1, 0, ctx->stream>>>(a.ctl);
     }
     PHEM_CUDA_TRY(cudaGetLastError());
     return PHEM_OK;
