@@ -276,6 +276,26 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32
                  : "memory");
 }
 
+// L2 policy for data read once (streamed inputs): evict first, so the
+// streams do not push small, reused arrays (parent, best) out of L2.
+__device__ __forceinline__ uint64_t l2_evict_first()
+{
+    uint64_t policy;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
+    return policy;
+}
+
+// bulk_copy_g2s with an L2 cache policy for the source.
+__device__ __forceinline__ void bulk_copy_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                                   uint64_t policy)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+        : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;

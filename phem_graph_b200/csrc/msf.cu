@@ -332,6 +332,7 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
     const uint32_t thr_hi = (uint32_t)(thr >> 32), thr_lo = (uint32_t)thr;
     const bool light_round = src == kSrcLight;
     const bool from_e0 = src != kSrcList;
+    const uint64_t stream_policy = l2_evict_first();  // inputs and lists are read once per pass
     const uint64_t count = from_e0 ? a.m : ctl->wl_len[r - 1];
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
     uint4 *out = (r & 1) ? a.wl1 : a.wl0;       // WL[r & 1]
@@ -357,8 +358,8 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             const uint64_t t = blockIdx.x + (uint64_t)s * gridDim.x;
             if (t < full_tiles) {
                 mbar_arrive_expect_tx(&s_bar[s], tile_bytes);
-                bulk_copy_g2s(stage_mem + s * stage_bytes<ITEMS>(), src_base + t * tile_bytes, tile_bytes,
-                              &s_bar[s]);
+                bulk_copy_g2s_hint(stage_mem + s * stage_bytes<ITEMS>(), src_base + t * tile_bytes, tile_bytes,
+                                   &s_bar[s], stream_policy);
             }
         }
     }
@@ -452,8 +453,8 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             if (t2 < full_tiles) {
                 fence_proxy_async_smem();
                 mbar_arrive_expect_tx(&s_bar[s2], tile_bytes);
-                bulk_copy_g2s(stage_mem + s2 * stage_bytes<ITEMS>(), src_base + t2 * tile_bytes, tile_bytes,
-                              &s_bar[s2]);
+                bulk_copy_g2s_hint(stage_mem + s2 * stage_bytes<ITEMS>(), src_base + t2 * tile_bytes, tile_bytes,
+                                   &s_bar[s2], stream_policy);
             }
         }
         if (warp == 0) {
@@ -522,7 +523,6 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             uint4 rec[4];
             bool on[4];
             unsigned long long key[4], ga[4], gb[4];
-#pragma unroll
             unsigned long long *ka[4], *kb[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -539,6 +539,8 @@ __global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
             }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
+                if (i0 + q * kBlock + warp * 32 >= total)
+                    continue;  // warp-uniform: no survivor in this warp's row (sparse input passes)
                 const uint32_t i = i0 + q * kBlock + threadIdx.x;
                 if (on[q])
                     out[i < split ? base + i : base2 + (i - split)] = rec[q];
