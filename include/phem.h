@@ -120,10 +120,10 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *                           (a prefix of the list), compresses, then the
  *                           rest; 0 unites all at once                     [0]
  *   "batch.block_size"      threads per CTA of the batched kernel,
- *                           256, 512 or 1024                               [512]
- *   "batch.items"           records per thread per step, 1, 2 or 4         [2]
+ *                           256, 512 or 1024                               [1024]
+ *   "batch.items"           records per thread per step, 1, 2 or 4         [4]
  *   "batch.compact_ratio"   a batched list pass compacts when the live
- *                           records are at most this share of the list     [0.5]
+ *                           records are at most this share of the list     [1.0]
  * None of them changes a result. */
 phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double value);
 phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *value);

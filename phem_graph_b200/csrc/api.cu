@@ -22,8 +22,7 @@ thread_local char g_last_error[512] = "";
 
 const char *const kKernelNames[kKernelCount] = {
     "msf_init", "msf_select", "msf_edge_pass", "msf_hook", "msf_compress", "msf_advance", "msf_gather",
-    "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "csr_pack",
-    "batch_solve"};
+    "cc_init", "cc_unite", "cc_merge", "cc_label", "cc_minid", "cc_count", "csr_to_coo", "batch_solve"};
 
 constexpr size_t kLaunchLogCap = 1u << 16;
 
@@ -765,10 +764,10 @@ phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const 
     // The converted edge list lives in a device buffer of its own so the MSF
     // solve can size the workspace freely.
     const size_t ob = (size_t)(n + 1) * sizeof(int64_t), cb = (size_t)nnz * sizeof(uint32_t),
-                 pb = (size_t)nnz * sizeof(uint64_t), wb = (size_t)m_upper * sizeof(uint32_t),
+                 tb = csr_scratch_bytes(nnz), wb = (size_t)m_upper * sizeof(uint32_t),
                  rb = (size_t)m_upper * sizeof(phem_edge);
-    const size_t o_off = 0, o_col = align256(ob), o_w = o_col + align256(cb), o_pk = o_w + align256(wb),
-                 o_rec = o_pk + align256(pb);
+    const size_t o_off = 0, o_col = align256(ob), o_w = o_col + align256(cb), o_tr = o_w + align256(wb),
+                 o_rec = o_tr + tb;
     void *buf = nullptr;
     if (cudaMalloc(&buf, o_rec + align256(rb) + 256) != cudaSuccess) {
         cudaGetLastError();
@@ -786,9 +785,10 @@ phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const 
     const int64_t *d_off = static_cast<const int64_t *>(put(offsets, ob, o_off));
     const uint32_t *d_col = static_cast<const uint32_t *>(put(cols, cb, o_col));
     const uint32_t *d_w = static_cast<const uint32_t *>(put(weights, wb, o_w));
-    uint64_t *d_pk = reinterpret_cast<uint64_t *>(b + o_pk);
+    uint32_t *d_tr = reinterpret_cast<uint32_t *>(b + o_tr);
     phem_edge *d_rec = reinterpret_cast<phem_edge *>(b + o_rec);
-    phem_status st = csr_launch_to_coo(ctx, d_off, d_col, (int32_t)n, nnz, d_pk);
+    // one pass: kept entry p becomes the record {row, col, weights[p]}
+    phem_status st = csr_launch_to_coo(ctx, d_off, d_col, (int32_t)n, nnz, d_tr, nullptr, d_w, d_rec, m_upper);
     if (st == PHEM_OK && cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost,
                                          ctx->stream) != cudaSuccess)
         st = PHEM_ERR_CUDA;
@@ -801,8 +801,6 @@ phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const 
                   (unsigned long long)ctx->h_ctl->misc[2], (unsigned long long)m_upper);
         st = PHEM_ERR_INVALID;
     }
-    if (st == PHEM_OK)
-        st = csr_launch_pack_records(ctx, d_pk, d_w, m_upper, d_rec);
     if (st == PHEM_OK)
         st = msf_common(ctx, d_rec, m_upper, n, msf, count, total, stats, nullptr);
     cudaStreamSynchronize(ctx->stream);
@@ -828,7 +826,9 @@ phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uin
     }
     const size_t ob = (size_t)(n + 1) * sizeof(int64_t), cb = (size_t)nnz * sizeof(uint32_t),
                  xb = (size_t)nnz * sizeof(uint64_t);
-    const size_t o_off = 0, o_col = align256(ob), o_out = o_col + align256(cb);
+    const size_t o_off = 0, o_col = align256(ob), o_tr = o_col + align256(cb),
+                 o_out = o_tr + csr_scratch_bytes(nnz);
+    auto scratch = [&] { return reinterpret_cast<uint32_t *>(static_cast<char *>(ctx->ws) + o_tr); };
     PHEM_TRY(ws_reserve(ctx, o_out + align256(xb / 2 + 16)));
     Staged so, sc, sx;
     PHEM_TRY(stage_in(ctx, offsets, ob, o_off, &so));
@@ -838,7 +838,7 @@ phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uin
     // in a symmetric CSR; a non-symmetric one may keep more, so count first in that case)
     if (sx.host) {
         PHEM_TRY(csr_launch_to_coo(ctx, static_cast<const int64_t *>(so.dev), static_cast<const uint32_t *>(sc.dev),
-                                   n, nnz, nullptr));
+                                   n, nnz, scratch(), nullptr));
         PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
         PHEM_TRY(stream_wait(ctx));
         const uint64_t kept = ctx->h_ctl->misc[2];
@@ -851,7 +851,7 @@ phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uin
         }
     }
     PHEM_TRY(csr_launch_to_coo(ctx, static_cast<const int64_t *>(so.dev), static_cast<const uint32_t *>(sc.dev), n,
-                               nnz, static_cast<uint64_t *>(sx.dev)));
+                               nnz, scratch(), static_cast<uint64_t *>(sx.dev)));
     PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
     PHEM_TRY(stream_wait(ctx));
     PHEM_TRY(ctl_status(ctx->h_ctl->err, "csr_to_coo"));

@@ -15,7 +15,7 @@ namespace phem {
 // Kernels the library launches; the profile reports them by these names.
 enum KernelId : int {
     kKInit = 0, kKSelect, kKEdgePass, kKHook, kKCompress, kKAdvance, kKGather,
-    kKCcInit, kKCcUnite, kKCcMerge, kKCcLabel, kKMinid, kKCcCount, kKCsrCoo, kKPack, kKBatch,
+    kKCcInit, kKCcUnite, kKCcMerge, kKCcLabel, kKMinid, kKCcCount, kKCsrCoo, kKBatch,
     kKernelCount
 };
 extern const char *const kKernelNames[kKernelCount];
@@ -51,9 +51,9 @@ struct phem_context {
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
     int tune_first_batch = 8;            // Boruvka rounds queued before the first host check
     int tune_next_batch = 4;             // rounds queued per later check
-    int tune_batch_block = 512;          // batched kernel: threads per CTA
-    int tune_batch_items = 2;            // batched kernel: records per thread per step
-    double tune_batch_compact = 0.5;     // batched kernel: compaction threshold
+    int tune_batch_block = 1024;         // batched kernel: threads per CTA
+    int tune_batch_items = 4;            // batched kernel: records per thread per step
+    double tune_batch_compact = 1.0;     // batched kernel: compaction threshold
     double tune_cc_sample = 0.0;         // CC: edges per vertex united before a compress (0: one pass)
     // launch accounting and optional per-kernel CUDA-event timing
     uint64_t launches[phem::kKernelCount] = {};
@@ -259,12 +259,15 @@ phem_status cc_launch_minid_labels(phem_context *ctx, int32_t n, uint32_t *paren
 phem_status cc_launch_count(phem_context *ctx, int32_t n, const int32_t *label, const uint64_t *forest);
 
 // ---- CSR (csr.cu) ----
+// Device scratch the conversion needs for nnz entries (per-tile rows, counts
+// and offsets).
+size_t csr_scratch_bytes(int64_t nnz);
 // Queues the conversion of a device CSR with nnz entries; the kept count lands
-// in ctx->ctl->misc[2].
+// in ctx->ctl->misc[2].  With records set, the kept entry at position p is
+// written as {row, col, w[p]} to records[p] for p < cap (out is ignored);
+// otherwise packed pairs go to out, or only the count when out is null.
 phem_status csr_launch_to_coo(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, int32_t n,
-                              int64_t nnz, uint64_t *out);
-// {u, v, w} records from packed pairs and per-edge weights.
-phem_status csr_launch_pack_records(phem_context *ctx, const uint64_t *pairs, const uint32_t *w, uint64_t m,
-                                    phem_edge *out);
+                              int64_t nnz, uint32_t *scratch, uint64_t *out, const uint32_t *w = nullptr,
+                              phem_edge *records = nullptr, uint64_t cap = 0);
 
 }  // namespace phem

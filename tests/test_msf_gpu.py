@@ -155,6 +155,77 @@ def test_csr_input(ctx):
     assert_msf(r, E, ids, cnt, tot)
 
 
+def _csr_from_entries(rows, cols, n):
+    """CSR of directed entries (rows need not be sorted; a row keeps its
+    entries in the given order)."""
+    order = np.argsort(rows, kind="stable")
+    off = np.zeros(n + 1, np.int64)
+    off[1:] = np.cumsum(np.bincount(rows, minlength=n))
+    return off, np.ascontiguousarray(np.asarray(cols)[order], np.uint32)
+
+
+def _csr_case(kind):
+    rng = np.random.default_rng(17)
+    if kind == "sparse_rows":  # long runs of empty rows between and after the entries
+        n = 1 << 20
+        u = rng.integers(0, n // 2, 3000)
+        v = rng.integers(0, n // 2, 3000)
+        return _csr_from_entries(np.r_[u, v], np.r_[v, u], n) + (n,)
+    if kind == "hub":  # one row spans many tiles
+        n = 40000
+        u = np.r_[np.full(20000, 5), rng.integers(0, n, 60000)]
+        v = np.r_[rng.permutation(np.arange(1, 20001)), rng.integers(0, n, 60000)]
+        return _csr_from_entries(np.r_[u, v], np.r_[v, u], n) + (n,)
+    if kind == "tile_edges":  # row lengths at and around the 1024-entry tile
+        lens = np.array([1024, 1023, 1025, 1, 2048, 0, 0, 1024, 3, 4096, 1022], np.int64)
+        n = 8192
+        rows = np.repeat(np.arange(len(lens)), lens)
+        cols = rng.integers(0, n, len(rows))
+        return _csr_from_entries(rows, cols, n) + (n,)
+    if kind == "asymmetric":  # directed entries, duplicates, self-loops, unsorted rows
+        n = 5000
+        u = rng.integers(0, n, 70000)
+        v = np.where(rng.random(70000) < 0.05, u, rng.integers(0, n, 70000))
+        return _csr_from_entries(u, v, n) + (n,)
+    if kind == "tiny":
+        return np.array([0, 1, 2, 2], np.int64), np.array([1, 0], np.uint32), 3
+    if kind == "empty":
+        return np.zeros(9, np.int64), np.zeros(0, np.uint32), 8
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("kind", ["sparse_rows", "hub", "tile_edges", "asymmetric", "tiny", "empty"])
+def test_csr_shapes(ctx, kind):
+    """csr_to_coo order and content equal the reference's row walk for empty
+    rows, rows spanning many tiles, tile-boundary rows and non-symmetric
+    input; the fused CSR MSF input numbers edges the same way."""
+    off, cols, n = _csr_case(kind)
+    want = oracle.csr_to_coo(off, cols, n)
+    np.testing.assert_array_equal(ctx.csr_to_coo(off, cols, n), want)
+    m = len(want)
+    w = np.random.default_rng(3).integers(1, 1 << 20, max(m, 1)).astype(np.uint32)[:m]
+    E = np.zeros((m, 3), np.uint32)
+    E[:, 0], E[:, 1], E[:, 2] = want >> np.uint64(32), want & np.uint64(0xFFFFFFFF), w
+    ids, cnt, tot = expect(E, n)
+    r = ctx.msf_solve_csr(off, cols, n, np.ascontiguousarray(w) if m else np.zeros(1, np.uint32), m)
+    assert_msf(r, E, ids, cnt, tot)
+
+
+def test_csr_device_buffers(ctx):
+    """Device offsets/cols/output take the no-staging path."""
+    import torch
+    g = gen.rmat_graph(15, 16, seed=8)
+    off, cols = gen.csr_from_pairs(g.pairs, g.n)
+    d_off = torch.from_numpy(off).cuda()
+    d_cols = torch.from_numpy(cols.view(np.int32)).cuda()
+    d_out = torch.empty(len(cols), dtype=torch.int64, device="cuda")
+    k = _lib.C.c_int64()
+    _lib.check(_lib.lib().phem_csr_to_coo(ctx._h, d_off.data_ptr(), d_cols.data_ptr(), g.n, d_out.data_ptr(),
+                                          _lib.C.byref(k)), "phem_csr_to_coo")
+    got = d_out[: k.value].cpu().numpy().view(np.uint64)
+    np.testing.assert_array_equal(got, g.pairs)
+
+
 def test_repeated_solves_share_context(ctx):
     """Workspace reuse across sizes, both directions."""
     for scale in (14, 10, 15, 9):
