@@ -19,6 +19,8 @@ Workload (one "step" = one full minimum-spanning-forest solve):
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl phem|reference]
 
 On one GPU the same JSON line also carries the metric's other workloads:
+  csr_input  the same R-MAT solve fed as its symmetrised CSR (int64 offsets,
+           uint32 columns) and per-edge weights, converted on the device;
   cc       connected components + forest, Erdos-Renyi n = 2^20, 8 * 2^20 draws;
   batched  4096 small graphs (ER and geometric) in one persistent launch,
            against one solve per graph;
@@ -237,6 +239,52 @@ def bench_cc(ctx, torch, peaks: dict, steps: int, warmup: int, cpu: bool) -> dic
                                               "median of 3 after 1 warm-up, call time only"}
             ref.close()
     return line
+
+
+def bench_csr_input(ctx, torch, g, steps: int, warmup: int, expect: tuple) -> dict:
+    """The same R-MAT solve fed as the symmetrised CSR of the workload (int64
+    offsets, uint32 columns) with one uint32 weight per edge: phem_msf_solve_csr
+    with device-resident CSR and forest, which converts the CSR on the device
+    (edge ids in row-walk order) and solves; per-kernel event times give the
+    conversion's share."""
+    import ctypes as C
+
+    from phem_graph_b200 import _lib, gen
+    off, cols = gen.csr_from_pairs(g.pairs, g.n)
+    dev = torch.device("cuda", ctx.device)
+    d_off = torch.from_numpy(off).to(dev)
+    d_cols = torch.from_numpy(cols.view(np.int32)).to(dev)
+    d_w = torch.from_numpy(g.w.view(np.int32)).to(dev)
+    d_out = torch.empty((g.n, 3), dtype=torch.int32, device=dev)
+    cnt, tot = C.c_uint64(), C.c_uint64()
+
+    def solve():
+        _lib.check(_lib.lib().phem_msf_solve_csr(ctx.handle, d_off.data_ptr(), d_cols.data_ptr(), g.n,
+                                                 d_w.data_ptr(), g.m, d_out.data_ptr(), C.byref(cnt), C.byref(tot),
+                                                 None), "phem_msf_solve_csr")
+
+    for _ in range(warmup):
+        solve()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        solve()  # returns after the count and total are on the host
+    t = (time.perf_counter() - t0) / steps
+    ctx.profile_reset()
+    ctx.set_profiling(True)
+    solve()
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    conv = prof.get("csr_to_coo", {})
+    del d_off, d_cols, d_w, d_out
+    torch.cuda.empty_cache()
+    nnz = len(cols)
+    return {"workload": f"msf_rmat_csr_nnz{nnz}", "n": g.n, "m": g.m, "csr_entries": nnz, "unit": UNIT,
+            "value": g.m / t / 1e9, "ms_per_solve": t * 1e3,
+            "csr_to_coo_ms": conv.get("total_ms"), "csr_to_coo_launches": conv.get("launches"),
+            "csr_to_coo_bytes": 4 * nnz + 8 * (g.n + 1) + 16 * g.m,
+            "result_matches_edge_list_solve": (cnt.value, tot.value) == expect,
+            "api": "phem_msf_solve_csr (C ABI), device CSR, weights and forest; host count and total"}
 
 
 def bench_batched(ctx, torch, num_graphs: int = 4096) -> dict:
@@ -625,6 +673,8 @@ def main() -> None:
         # the other workloads of the metric, measured after the headline run
         del d_edges, d_out
         torch.cuda.empty_cache()
+        line["csr_input"] = bench_csr_input(ctx, torch, g, max(3, args.steps // 2), args.warmup,
+                                            (stats.count, stats.total))
         line["cc"] = bench_cc(ctx, torch, peaks, args.steps, args.warmup, not args.no_cpu_baseline)
         line["batched"] = bench_batched(ctx, torch)
         line["served"] = bench_served(torch)

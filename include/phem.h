@@ -118,7 +118,7 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.edge_items"        records per thread in the edge pass, 4 or 8   [8]
  *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
  *                           (a prefix of the list), compresses, then the
- *                           rest; 0 unites all at once                     [0]
+ *                           rest; 0 unites all at once                     [1]
  *   "batch.block_size"      threads per CTA of the batched kernel,
  *                           256, 512 or 1024                               [1024]
  *   "batch.items"           records per thread per step, 1, 2 or 4         [4]
@@ -128,7 +128,8 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
 phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double value);
 phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *value);
 
-/* Releases the context's device workspace (it grows on demand otherwise). */
+/* Releases the context's device workspace and converted-input buffer (both
+ * grow on demand otherwise). */
 phem_status phem_context_trim(phem_context *ctx);
 
 const char *phem_status_string(phem_status s);

@@ -114,30 +114,41 @@ uint64_t next_epochs(phem_context *ctx, uint32_t count)
     return e;
 }
 
-phem_status ws_reserve(phem_context *ctx, size_t bytes)
+// Grows a grow-only device buffer to at least `bytes` (contents are not kept).
+static phem_status grow_buffer(phem_context *ctx, void **buf, size_t *have, size_t bytes, const char *what)
 {
-    if (bytes <= ctx->ws_bytes)
+    if (bytes <= *have)
         return PHEM_OK;
     PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    if (ctx->ws) {
-        cudaFree(ctx->ws);
-        ctx->ws = nullptr;
-        ctx->ws_bytes = 0;
+    if (*buf) {
+        cudaFree(*buf);
+        *buf = nullptr;
+        *have = 0;
     }
     const size_t want = bytes + bytes / 8;  // some headroom against small growth steps
-    if (cudaMalloc(&ctx->ws, want) != cudaSuccess) {
+    if (cudaMalloc(buf, want) != cudaSuccess) {
         cudaGetLastError();
-        if (cudaMalloc(&ctx->ws, bytes) != cudaSuccess) {
+        if (cudaMalloc(buf, bytes) != cudaSuccess) {
             cudaGetLastError();
-            ctx->ws = nullptr;
-            set_error("workspace: cannot allocate %zu bytes", bytes);
+            *buf = nullptr;
+            set_error("%s: cannot allocate %zu bytes", what, bytes);
             return PHEM_ERR_NOMEM;
         }
-        ctx->ws_bytes = bytes;
+        *have = bytes;
         return PHEM_OK;
     }
-    ctx->ws_bytes = want;
+    *have = want;
     return PHEM_OK;
+}
+
+phem_status ws_reserve(phem_context *ctx, size_t bytes)
+{
+    return grow_buffer(ctx, &ctx->ws, &ctx->ws_bytes, bytes, "workspace");
+}
+
+phem_status input_reserve(phem_context *ctx, size_t bytes)
+{
+    return grow_buffer(ctx, &ctx->input, &ctx->input_bytes, bytes, "converted input");
 }
 
 phem_status status_reserve(phem_context *ctx, size_t words)
@@ -285,6 +296,8 @@ void phem_context_destroy(phem_context *ctx)
         cudaStreamSynchronize(ctx->stream);
     if (ctx->ws)
         cudaFree(ctx->ws);
+    if (ctx->input)
+        cudaFree(ctx->input);
     if (ctx->status)
         cudaFree(ctx->status);
     if (ctx->ctl)
@@ -462,6 +475,10 @@ phem_status phem_context_trim(phem_context *ctx)
         cudaFree(ctx->ws);
     ctx->ws = nullptr;
     ctx->ws_bytes = 0;
+    if (ctx->input)
+        cudaFree(ctx->input);
+    ctx->input = nullptr;
+    ctx->input_bytes = 0;
     return PHEM_OK;
 }
 
@@ -761,20 +778,15 @@ phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const 
         set_error("msf_solve_csr: offsets[n] = %lld out of range", (long long)nnz);
         return PHEM_ERR_INVALID;
     }
-    // The converted edge list lives in a device buffer of its own so the MSF
-    // solve can size the workspace freely.
+    // The converted edge list lives in the context's grow-only input buffer
+    // (not the workspace, which the MSF solve sizes freely).
     const size_t ob = (size_t)(n + 1) * sizeof(int64_t), cb = (size_t)nnz * sizeof(uint32_t),
                  tb = csr_scratch_bytes(nnz), wb = (size_t)m_upper * sizeof(uint32_t),
                  rb = (size_t)m_upper * sizeof(phem_edge);
     const size_t o_off = 0, o_col = align256(ob), o_w = o_col + align256(cb), o_tr = o_w + align256(wb),
                  o_rec = o_tr + tb;
-    void *buf = nullptr;
-    if (cudaMalloc(&buf, o_rec + align256(rb) + 256) != cudaSuccess) {
-        cudaGetLastError();
-        set_error("msf_solve_csr: cannot allocate the edge list");
-        return PHEM_ERR_NOMEM;
-    }
-    char *b = static_cast<char *>(buf);
+    PHEM_TRY(input_reserve(ctx, o_rec + align256(rb) + 256));
+    char *b = static_cast<char *>(ctx->input);
     auto put = [&](const void *src, size_t bytes, size_t off) -> const void * {
         if (is_device_ptr(src))
             return src;
@@ -803,8 +815,6 @@ phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const 
     }
     if (st == PHEM_OK)
         st = msf_common(ctx, d_rec, m_upper, n, msf, count, total, stats, nullptr);
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(buf);
     return st;
 }
 

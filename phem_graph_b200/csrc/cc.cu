@@ -11,9 +11,14 @@
 //   * edges are read four at a time with 128-bit streaming loads
 //     (evict-first), so the 8 B/edge stream does not push the parent array
 //     out of L2;
-//   * find() uses path halving with L2-coherent loads (ld.global.cg): a hook
-//     made by another SM is seen at once, and no stale L1 line can make a
-//     retry loop spin;
+//   * a union first compares the endpoints' parents (two loads settle most
+//     edges once trees are flat), then walks both roots in lockstep so the
+//     two walks' loads overlap, stopping early where the walks meet; the
+//     first walk reads through L1, a walk after a failed CAS through L2;
+//   * path halving writes are atomic mins: ids fall towards the root, so a
+//     walk working from a stale parent never undoes another walk's shortcut;
+//   * phem_cc_solve unites a prefix of about one edge per vertex, points
+//     every vertex at its root, then unites the rest (cc.sample_per_vertex);
 //   * every loop is bounded; a bound that trips sets a status bit instead of
 //     hanging the GPU.
 #include <algorithm>
@@ -38,25 +43,84 @@ __device__ __forceinline__ int32_t ld_ca(const int32_t *p)
 
 // Root of x with path halving.  Writes only touch non-roots (a vertex that is
 // not a root never becomes one again), so they cannot race with the CAS that
-// hooks a root; each write points a vertex at one of its ancestors.  A path
+// hooks a root; each write points a vertex at one of its ancestors, as a
+// fire-and-forget atomic min.  A path
 // has fewer than n + 1 vertices, so n + 1 steps bound the walk.  CACHED walks
 // read through L1 (see ld_ca); the others read L2-coherently.
+// Vertex 0 is always a root (nothing is smaller to hook it under), so a walk
+// that reaches it stops without reading the word every walk would read.
 template <bool CACHED>
 __device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x, int32_t n, uint32_t *err)
 {
     const uint32_t cap = (uint32_t)n + 1;
     for (uint32_t steps = 0; steps < cap; steps++) {
         const int32_t p = CACHED ? ld_ca(parent + x) : __ldcg(parent + x);
-        if (p == x)
-            return x;
+        if (p == x || p == 0)
+            return p;
         const int32_t gp = CACHED ? ld_ca(parent + p) : __ldcg(parent + p);
         if (gp == p)
             return p;
-        parent[x] = gp;
+        // ids fall towards the root (hooks point at smaller ids), so a min
+        // never moves x's pointer back below a shortcut another walk made
+        // after this one read a (possibly stale) parent
+        atomicMin(parent + x, gp);
         x = gp;
     }
     set_err(err, kErrChase);
     return x;
+}
+
+// The roots of a and b, walked in lockstep (both walks' loads are in flight
+// together) with the same halving as uf_find.  Returns true as soon as the
+// walks meet (one component; *ra, *rb are then not set), else false with
+// the two roots.
+template <bool CACHED>
+__device__ __forceinline__ bool uf_find2(int32_t *parent, int32_t a, int32_t b, int32_t n, uint32_t *err,
+                                         int32_t *ra, int32_t *rb)
+{
+    const uint32_t cap = (uint32_t)n + 1;
+    bool da = false, db = false;  // walk finished at a root
+    for (uint32_t steps = 0; steps < cap; steps++) {
+        if (a == b)
+            return true;
+        if (da && db) {
+            *ra = a;
+            *rb = b;
+            return false;
+        }
+        const int32_t pa = da ? a : (CACHED ? ld_ca(parent + a) : __ldcg(parent + a));
+        const int32_t pb = db ? b : (CACHED ? ld_ca(parent + b) : __ldcg(parent + b));
+        const bool ra_now = !da && (pa == a || pa == 0), rb_now = !db && (pb == b || pb == 0);
+        const bool step_a = !da && !ra_now, step_b = !db && !rb_now;
+        const int32_t ga = step_a ? (CACHED ? ld_ca(parent + pa) : __ldcg(parent + pa)) : pa;
+        const int32_t gb = step_b ? (CACHED ? ld_ca(parent + pb) : __ldcg(parent + pb)) : pb;
+        if (ra_now) {
+            a = pa;
+            da = true;
+        } else if (step_a) {
+            if (ga == pa) {
+                da = true;
+            } else {
+                atomicMin(parent + a, ga);
+            }
+            a = ga;
+        }
+        if (rb_now) {
+            b = pb;
+            db = true;
+        } else if (step_b) {
+            if (gb == pb) {
+                db = true;
+            } else {
+                atomicMin(parent + b, gb);
+            }
+            b = gb;
+        }
+    }
+    set_err(err, kErrChase);
+    *ra = a;
+    *rb = b;
+    return a == b;
 }
 
 // One union with the reference's hook rule (larger root under smaller root,
@@ -75,8 +139,9 @@ __device__ __forceinline__ bool uf_unite(int32_t *parent, unsigned long long *fo
     }
     for (uint32_t retry = 0; retry < kUnionRetryCap; retry++) {
         // first attempt through L1; after a failed CAS, coherent walks
-        const int32_t ru = retry == 0 ? uf_find<true>(parent, u, n, err) : uf_find<false>(parent, u, n, err);
-        const int32_t rv = retry == 0 ? uf_find<true>(parent, v, n, err) : uf_find<false>(parent, v, n, err);
+        int32_t ru, rv;
+        if (retry == 0 ? uf_find2<true>(parent, u, v, n, err, &ru, &rv) : uf_find2<false>(parent, u, v, n, err, &ru, &rv))
+            return false;
         if (ru == rv)
             return false;
         if ((retry & 63) == 63 && (*(volatile uint32_t *)err & (kErrChase | kErrRetry)))

@@ -113,7 +113,7 @@ __device__ __forceinline__ uint32_t resolve_rows(int64_t first, int64_t nnz, int
     const uint32_t le = 0xffffffffu >> (31 - lane);  // lanes 0..lane
     const int64_t j0 = first + warp * kCsrSeg + lane;
     uint32_t *mk = s_mark + warp * kCsrSeg + lane;
-    uint32_t carry = max(s_seg[warp], (uint32_t)row0), keep = 0, n_kept = 0;
+    uint32_t carry = max(s_seg[warp], (uint32_t)row0), keep = 0;
     __syncwarp();
     if (lane == 0)
         s_seg[warp] = 0;
@@ -125,10 +125,12 @@ __device__ __forceinline__ uint32_t resolve_rows(int64_t first, int64_t nnz, int
         const uint32_t v = __shfl_sync(0xffffffffu, m, b ? 31 - __clz(b) : 0);
         row[k] = b ? v : carry;
         carry = __shfl_sync(0xffffffffu, row[k], 31);
-        const bool kp = j0 + 32 * k < nnz && (int64_t)row[k] < (int64_t)col[k];
-        keep |= (uint32_t)kp << k;
-        n_kept += __popc(__ballot_sync(0xffffffffu, kp));
+        keep |= (uint32_t)(j0 + 32 * k < nnz && (int64_t)row[k] < (int64_t)col[k]) << k;
     }
+    uint32_t n_kept = __popc(keep);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+        n_kept += __shfl_xor_sync(0xffffffffu, n_kept, d);
     *kept = n_kept;
     return keep;
 }

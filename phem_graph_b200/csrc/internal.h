@@ -34,6 +34,8 @@ struct phem_context {
     cudaStream_t copy_stream = nullptr;// second stream for overlapped host copies
     void *ws = nullptr;                // grow-only device workspace
     size_t ws_bytes = 0;
+    void *input = nullptr;             // grow-only buffer for converted inputs (CSR -> records)
+    size_t input_bytes = 0;
     uint64_t *status = nullptr;        // look-back status words, only ever written by look-back
     size_t status_words = 0;           // (zeroed when grown; epochs keep old words from matching)
     phem::Ctl *ctl = nullptr;          // device control block
@@ -54,7 +56,7 @@ struct phem_context {
     int tune_batch_block = 1024;         // batched kernel: threads per CTA
     int tune_batch_items = 4;            // batched kernel: records per thread per step
     double tune_batch_compact = 1.0;     // batched kernel: compaction threshold
-    double tune_cc_sample = 0.0;         // CC: edges per vertex united before a compress (0: one pass)
+    double tune_cc_sample = 1.0;         // CC: edges per vertex united before a compress (0: one pass)
     // launch accounting and optional per-kernel CUDA-event timing
     uint64_t launches[phem::kKernelCount] = {};
     double kernel_ms[phem::kKernelCount] = {};
@@ -101,6 +103,8 @@ struct Carve {
 
 // Ensures ws_bytes >= bytes (contents are not preserved when it grows).
 phem_status ws_reserve(phem_context *ctx, size_t bytes);
+// Ensures input_bytes >= bytes (the converted-input buffer; contents not preserved).
+phem_status input_reserve(phem_context *ctx, size_t bytes);
 // Ensures the look-back status array holds >= words entries.
 phem_status status_reserve(phem_context *ctx, size_t words);
 
