@@ -297,8 +297,10 @@ __host__ __device__ constexpr size_t pipe_smem()
     return kStages * stage_bytes<ITEMS>();
 }
 
+// Resident CTAs per SM: two for 8 records per thread (the three stages fill
+// shared memory), three for 4 (half the stage bytes; registers capped to fit).
 template <int KIND, int ITEMS>
-__global__ void __launch_bounds__(kBlock, 2) edge_pass_kernel(RoundArgs a)
+__global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(RoundArgs a)
 {
     constexpr int kCnt = ITEMS * kWarps;  // row/warp counts per tile
     extern __shared__ __align__(128) unsigned char stage_mem[];
@@ -672,33 +674,52 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     const uint64_t step = (uint64_t)gridDim.x * kBlock * kVItems;
     for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * kVItems; i0 < count; i0 += step) {
-        bool stays[kVItems];
-        uint32_t x[kVItems];
+        bool stays[kVItems], active[kVItems], walking[kVItems];
+        uint32_t x[kVItems], y[kVItems], y0[kVItems];
+        // the candidates' loads and root walks advance in lockstep, so their
+        // dependent loads are in flight together
 #pragma unroll
         for (int k = 0; k < kVItems; k++) {
             const uint64_t i = i0 + k * kBlock + threadIdx.x;
-            const bool in = i < count;
-            x[k] = in ? ((all || full) ? (uint32_t)i : cand[i]) : 0;
-            const bool active = in && (full || a.best[x[k]] != kKeyNone);
+            active[k] = i < count;
+            x[k] = active[k] ? ((all || full) ? (uint32_t)i : cand[i]) : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < kVItems; k++)
+            active[k] = active[k] && (full || a.best[x[k]] != kKeyNone);
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
+            y0[k] = y[k] = active[k] ? a.parent[x[k]] : x[k];
+            walking[k] = active[k];
+        }
+        for (uint32_t steps = 0;; steps++) {
+            uint32_t p[kVItems];
+#pragma unroll
+            for (int k = 0; k < kVItems; k++)
+                p[k] = walking[k] ? a.parent[y[k]] : y[k];
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < kVItems; k++) {
+                walking[k] = walking[k] && p[k] != y[k];
+                y[k] = p[k];
+                any |= walking[k];
+            }
+            if (!any)
+                break;
+            if (steps > a.n) {
+                set_err(&ctl->err, kErrChase);
+                break;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kVItems; k++) {
             stays[k] = false;
-            if (active) {
-                uint32_t y = a.parent[x[k]];
-                uint32_t steps = 0;
-                for (;;) {
-                    const uint32_t p = a.parent[y];
-                    if (p == y)
-                        break;
-                    y = p;
-                    if (++steps > a.n) {
-                        set_err(&ctl->err, kErrChase);
-                        break;
-                    }
-                }
-                if (a.parent[x[k]] != y)
-                    a.parent[x[k]] = y;
+            if (active[k]) {
+                if (y0[k] != y[k])
+                    a.parent[x[k]] = y[k];
                 if (!full) {
                     a.best[x[k]] = kKeyNone;
-                    stays[k] = (y == x[k]);
+                    stays[k] = (y[k] == x[k]);
                 }
             }
         }
@@ -929,7 +950,9 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
     }
     {
         KernelScope k(ctx, kKCompress);
-        compress_kernel<<<vb, kBlock, 0, ctx->stream>>>(a);
+        // four CTAs per SM: enough walks in flight for the all-vertex rounds,
+        // and a short launch for the late rounds' few candidates
+        compress_kernel<<<std::min(vb, ctx->sm_count * 4), kBlock, 0, ctx->stream>>>(a);
     }
     PHEM_CUDA_TRY(cudaGetLastError());
     return PHEM_OK;
