@@ -1,8 +1,9 @@
 // noalloc.cu -- connected components + spanning forest without allocating.
 //
-// phem_cc_solve_noalloc runs the union-find of phem_cc_solve's default path
-// (the reference's init_parent_label_T1edges + union_find_gpu_COO + cc,
-// CC/ExternalSpanningTree.cu:77-116, CC/GPUSpanningTree.cu:122-128) with its
+// phem_cc_solve_noalloc runs a one-pass union-find with phem_cc_solve's hook
+// rule, so its labels and forest mean the same (the reference's
+// init_parent_label_T1edges + union_find_gpu_COO + cc,
+// CC/ExternalSpanningTree.cu:77-116, CC/GPUSpanningTree.cu:122-128), with its
 // parent array in a fixed-size file-scope device array instead of a context
 // workspace.  It exists for callers that cannot allocate device memory when
 // they need a solve:
