@@ -176,7 +176,10 @@ typedef struct phem_msf_stats {
  *                 PHEM_FOREST_EMPTY (forest may be NULL).
  * Edges with u >= v are skipped, as union_find_gpu_COO skips them
  * (CC/ExternalSpanningTree.cu:82).  Endpoints must be < n (else INVALID).
- * PHEM_CC_CANONICAL requires m < 2^32.  stats may be NULL. */
+ * PHEM_CC_CANONICAL requires m < 2^32.  stats may be NULL.
+ * Host edges (2^20 or more, default forest) are copied in chunks on a second
+ * stream, overlapped with the unions of earlier chunks; stats->device_ms then
+ * includes the copy. */
 phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, int32_t n,
                           int32_t *labels, uint64_t *forest, uint32_t flags, phem_cc_stats *stats);
 

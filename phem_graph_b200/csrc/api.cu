@@ -484,6 +484,63 @@ phem_status phem_context_trim(phem_context *ctx)
 
 // ------------------------------------------------------------------ CC
 
+// Host edges of at least this many are copied in chunks overlapped with the
+// unions (smaller inputs: one copy, then the unions).
+constexpr int64_t kOverlapMinEdges = 1 << 20;
+constexpr int64_t kOverlapChunkEdges = 1 << 21;  // 16 MB per copy
+
+// The default CC schedule (unite [0, s), compress, unite [s, m)) over host
+// edges: chunks are copied into d_stage on the copy stream, and each chunk's
+// union waits only for its own copy, so the link and the unions overlap.
+// Chunk boundaries are even, keeping every chunk 16-byte aligned for the
+// union's 128-bit loads.
+static phem_status cc_unite_overlapped(phem_context *ctx, const uint64_t *h_edges, uint64_t *d_stage, int64_t m,
+                                       int64_t s, int32_t n, int32_t *d_par, uint64_t *d_for)
+{
+    std::vector<std::pair<int64_t, int64_t>> chunks;  // (offset, count)
+    for (int64_t off = 0; off < s; off += kOverlapChunkEdges)
+        chunks.emplace_back(off, std::min(kOverlapChunkEdges, s - off));
+    const size_t prefix_chunks = chunks.size();
+    for (int64_t off = s; off < m; off += kOverlapChunkEdges)
+        chunks.emplace_back(off, std::min(kOverlapChunkEdges, m - off));
+    std::vector<cudaEvent_t> copied(chunks.size() + 1, nullptr);
+    phem_status st = PHEM_OK;
+    for (auto &e : copied)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            e = nullptr;
+            set_error("cc_solve: cannot create copy events");
+            st = PHEM_ERR_CUDA;
+        }
+    // the first copy waits for earlier work on the context stream, which may
+    // still read the staging area
+    if (st == PHEM_OK && (cudaEventRecord(copied.back(), ctx->stream) != cudaSuccess ||
+                          cudaStreamWaitEvent(ctx->copy_stream, copied.back(), 0) != cudaSuccess)) {
+        set_error("cc_solve: cannot order the copy stream");
+        st = PHEM_ERR_CUDA;
+    }
+    for (size_t c = 0; st == PHEM_OK && c < chunks.size(); c++) {
+        const int64_t off = chunks[c].first, cnt = chunks[c].second;
+        if (cudaMemcpyAsync(d_stage + off, h_edges + off, (size_t)cnt * sizeof(uint64_t), cudaMemcpyDefault,
+                            ctx->copy_stream) != cudaSuccess ||
+            cudaEventRecord(copied[c], ctx->copy_stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ctx->stream, copied[c], 0) != cudaSuccess) {
+            set_error("cc_solve: chunk copy failed: %s", cudaGetErrorString(cudaGetLastError()));
+            st = PHEM_ERR_CUDA;
+            break;
+        }
+        st = cc_launch_unite(ctx, d_stage + off, cnt, n, d_par, d_for);
+        if (st == PHEM_OK && c + 1 == prefix_chunks && s < m)
+            st = cc_launch_compress(ctx, n, d_par);
+    }
+    if (st != PHEM_OK)
+        cudaStreamSynchronize(ctx->copy_stream);  // no copy may still land in the workspace
+    for (auto e : copied)
+        if (e)
+            cudaEventDestroy(e);  // released once the work recorded on it completes
+    return st;
+}
+
 phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, int32_t n, int32_t *labels,
                           uint64_t *forest, uint32_t flags, phem_cc_stats *stats)
 {
@@ -511,12 +568,16 @@ phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, i
         PHEM_TRY(ws_reserve(ctx, extra));
     }
     Staged se, sl, sf;
-    const bool aligned_dev = is_device_ptr(edges) && (((uintptr_t)edges & 15) == 0);
+    const bool on_device = is_device_ptr(edges);
+    const bool aligned_dev = on_device && (((uintptr_t)edges & 15) == 0);
+    // large host inputs of the default path are copied in chunks, overlapped
+    // with the unions of the chunks before them
+    const bool overlap = !canonical && !on_device && m >= kOverlapMinEdges;
     if (aligned_dev) {
         se.dev = const_cast<uint64_t *>(edges);
     } else {
         se.dev = static_cast<char *>(ctx->ws) + base + o_edges;
-        if (m)
+        if (m && !overlap)
             PHEM_CUDA_TRY(cudaMemcpyAsync(se.dev, edges, eb, cudaMemcpyDefault, ctx->stream));
     }
     stage_out(ctx, labels, lb, base + o_lab, &sl);
@@ -543,10 +604,14 @@ phem_status phem_cc_solve(phem_context *ctx, const uint64_t *edges, int64_t m, i
         int64_t s = (int64_t)(ctx->tune_cc_sample * (double)n) & ~int64_t(1);
         if (s <= 0 || s >= m)
             s = m;
-        PHEM_TRY(cc_launch_unite(ctx, d_edges, s, n, d_par, d_for));
-        if (s < m) {
-            PHEM_TRY(cc_launch_compress(ctx, n, d_par));
-            PHEM_TRY(cc_launch_unite(ctx, d_edges + s, m - s, n, d_par, d_for));
+        if (overlap) {
+            PHEM_TRY(cc_unite_overlapped(ctx, edges, const_cast<uint64_t *>(d_edges), m, s, n, d_par, d_for));
+        } else {
+            PHEM_TRY(cc_launch_unite(ctx, d_edges, s, n, d_par, d_for));
+            if (s < m) {
+                PHEM_TRY(cc_launch_compress(ctx, n, d_par));
+                PHEM_TRY(cc_launch_unite(ctx, d_edges + s, m - s, n, d_par, d_for));
+            }
         }
         PHEM_TRY(cc_launch_label(ctx, n, d_par, d_lab));
     }

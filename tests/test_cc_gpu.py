@@ -205,6 +205,28 @@ def test_sample_schedule_same_labels(ctx, sample):
     check_forest(g.pairs, g.n, r.labels, r.forest)
 
 
+@pytest.mark.parametrize("sample", [0.0, 1.0, 6.0])
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_edges_copied_in_overlapped_chunks(ctx, sample, pinned):
+    """Large host inputs are copied in 2^21-edge chunks on a second stream,
+    each chunk's union waiting for its own copy; prefixes that end inside,
+    at the end of, or beyond several chunks give the oracle's labels and a
+    valid forest, from pageable and from pinned memory, twice in a row."""
+    import torch
+    g = gen.er_graph(1 << 19, 5_000_001, 17)
+    edges = g.pairs if not pinned else torch.from_numpy(g.pairs.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    want, _ = oracle.cc_solve(g.pairs, g.n)
+    saved = ctx.get_tuning("cc.sample_per_vertex")
+    try:
+        ctx.set_tuning("cc.sample_per_vertex", sample)
+        for _ in range(2):
+            r = ctx.cc_solve(edges, g.n)
+            np.testing.assert_array_equal(r.labels, want)
+            check_forest(g.pairs, g.n, r.labels, r.forest)
+    finally:
+        ctx.set_tuning("cc.sample_per_vertex", saved)
+
+
 def test_solves_from_reference_file_formats(ctx, tmp_path):
     """Inputs read from the reference drivers' file formats solve to the
     oracle's results (ECL binary CSR for CC, MatrixMarket for MSF)."""
