@@ -297,14 +297,25 @@ class Context:
 
     # ------------------------------------------------------------ batches
 
-    def batch_solve(self, batch, labels: bool = True) -> BatchResult:
-        """Every graph of a gen.Batch in one persistent launch."""
+    def batch_solve(self, batch, labels: bool = True, out: dict | None = None) -> BatchResult:
+        """Every graph of a gen.Batch in one persistent launch.  `out` may hold
+        caller arrays (for instance in pinned memory) for any of "ids" (uint32,
+        >= total vertices), "count" (uint32, >= graphs), "total" (uint64,
+        >= graphs) and "labels" (int32, >= total vertices)."""
         graphs, edges = _batch_args(batch)
         G, V = len(graphs), batch.total_vertices
-        ids = np.empty(max(V, 1), np.uint32)
-        cnt = np.empty(max(G, 1), np.uint32)
-        tot = np.empty(max(G, 1), np.uint64)
-        lab = np.empty(max(V, 1), np.int32) if labels else None
+        out = out or {}
+        ids = out["ids"] if "ids" in out else np.empty(max(V, 1), np.uint32)
+        cnt = out["count"] if "count" in out else np.empty(max(G, 1), np.uint32)
+        tot = out["total"] if "total" in out else np.empty(max(G, 1), np.uint64)
+        lab = None
+        if labels:
+            lab = out["labels"] if "labels" in out else np.empty(max(V, 1), np.int32)
+        for name, a, need, dt in (("ids", ids, V, np.uint32), ("count", cnt, G, np.uint32),
+                                  ("total", tot, G, np.uint64), ("labels", lab, V, np.int32)):
+            if a is not None and (a.dtype != dt or len(a) < need or not a.flags.c_contiguous):
+                raise ValueError(f"batch_solve: out[{name!r}] must be a contiguous {np.dtype(dt).name} array "
+                                 f"of at least {need} entries")
         st = BatchStats()
         check(lib().phem_batch_solve(self._h, ptr(graphs), G, ptr(edges), len(edges), V, ptr(ids), ptr(cnt),
                                      ptr(tot), ptr(lab), C.byref(st)), "phem_batch_solve")

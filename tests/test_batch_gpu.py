@@ -82,6 +82,28 @@ def test_mixed_batch_matches_oracle(ctx):
     check_batch(b, res)
 
 
+def test_caller_output_arrays(ctx):
+    """Results written into caller arrays (pinned, and larger than needed)
+    equal the ones the call allocates; a wrong dtype is refused."""
+    import torch
+    b = small_mixed(24, seed=7)
+    want = ctx.batch_solve(b)
+    V, G = b.total_vertices, b.num_graphs
+    out = {"ids": torch.empty(V + 5, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+           "count": torch.empty(G, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+           "total": torch.empty(G + 1, dtype=torch.int64).pin_memory().numpy().view(np.uint64),
+           "labels": torch.empty(V, dtype=torch.int32).pin_memory().numpy()}
+    for _ in range(2):
+        got = ctx.batch_solve(b, out=out)
+        np.testing.assert_array_equal(got.count, want.count)
+        np.testing.assert_array_equal(got.total, want.total)
+        np.testing.assert_array_equal(got.labels, want.labels)
+        for g in range(G):
+            np.testing.assert_array_equal(got.forest(b, g), want.forest(b, g))
+    with pytest.raises(ValueError):
+        ctx.batch_solve(b, out={"count": np.empty(G, np.int64)})
+
+
 def test_cc_kind_canonical_forest(ctx):
     b = small_mixed(32, seed=3, kind=gen.PHEM_BATCH_CC)
     res = ctx.batch_solve(b)
