@@ -385,32 +385,42 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
         const uint32_t id0 = (uint32_t)tbase;
         uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
         bool keep[ITEMS];
+        // Whole tiles are read from the stage with shared-memory loads (the
+        // branch is uniform over the tile); only the ragged last tile reads
+        // global memory.  Selecting one pointer from either space would make
+        // every record load a generic load.
+        if (from_e0) {
+            bool any_bad = false;
 #pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            const uint32_t idx = j * kBlock + threadIdx.x;
-            const bool inb = idx < rem;
-            id[j] = id0 + idx;
-            if (from_e0) {
+            for (int j = 0; j < ITEMS; j++) {
+                const uint32_t idx = j * kBlock + threadIdx.x;
+                const bool inb = idx < rem;
+                id[j] = id0 + idx;
                 uint32_t u = 0, v = 0, ww = 0;
-                if (inb) {
-                    if (KIND == kKindMsf) {
-                        const uint32_t *p = bulk ? reinterpret_cast<const uint32_t *>(stage) + 3 * idx
-                                                 : static_cast<const uint32_t *>(a.e0) + 3 * (tbase + idx);
+                if (KIND == kKindMsf) {
+                    if (bulk) {
+                        const uint32_t *p = reinterpret_cast<const uint32_t *>(stage) + 3 * idx;
                         u = p[0];
                         v = p[1];
                         ww = p[2];
-                    } else {
-                        const unsigned long long e = bulk
-                                                         ? reinterpret_cast<const unsigned long long *>(stage)[idx]
-                                                         : static_cast<const unsigned long long *>(a.e0)[tbase + idx];
-                        u = (uint32_t)(e >> 32);
-                        v = (uint32_t)e;
+                    } else if (inb) {
+                        const uint32_t *p = static_cast<const uint32_t *>(a.e0) + 3 * (tbase + idx);
+                        u = p[0];
+                        v = p[1];
+                        ww = p[2];
                     }
+                } else {
+                    unsigned long long e = 0;
+                    if (bulk)
+                        e = reinterpret_cast<const unsigned long long *>(stage)[idx];
+                    else if (inb)
+                        e = static_cast<const unsigned long long *>(a.e0)[tbase + idx];
+                    u = (uint32_t)(e >> 32);
+                    v = (uint32_t)e;
                 }
                 const bool live_e = inb && e0_live<KIND>(u, v);
                 const bool bad = live_e && max(u, v) >= a.n;
-                if (bad && light_round)
-                    set_err(&ctl->err, kErrRange);
+                any_bad |= bad;
                 // e0_key(w, id) < thr, compared as (high word, low word)
                 const bool light = KIND == kKindMsf ? (ww < thr_hi || (ww == thr_hi && id[j] < thr_lo))
                                                     : (thr_hi != 0 || id[j] < thr_lo);
@@ -418,10 +428,21 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
                 ra[j] = u;
                 rb[j] = v;
                 w[j] = ww;
-            } else {
+            }
+            if (any_bad && light_round)
+                set_err(&ctl->err, kErrRange);
+        } else {
+#pragma unroll
+            for (int j = 0; j < ITEMS; j++) {
+                const uint32_t idx = j * kBlock + threadIdx.x;
+                const bool inb = idx < rem;
                 uint4 rec = make_uint4(0, 0, 0, 0);
-                if (inb)
-                    rec = bulk ? reinterpret_cast<const uint4 *>(stage)[idx] : __ldcs(in + (tbase + idx));
+                if (bulk) {
+                    if (inb)
+                        rec = reinterpret_cast<const uint4 *>(stage)[idx];
+                } else if (inb) {
+                    rec = __ldcs(in + (tbase + idx));
+                }
                 keep[j] = inb;
                 ra[j] = rec.x;
                 rb[j] = rec.y;
