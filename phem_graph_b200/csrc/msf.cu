@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
         const unsigned below = (1u << lane) - 1u;
 #pragma unroll
         for (int j = 0; j < ITEMS; j++)
-            if (keep[j])
+            if (mask[j] && keep[j])  // mask: warp-uniform skip of rows without survivors
                 staging[s_cnt[j * kWarps + warp] + __popc(mask[j] & below)] = make_uint4(ra[j], rb[j], w[j], id[j]);
         __syncthreads();
         // Dense phase: coalesced survivor writes and the offers of both
@@ -547,10 +547,18 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
             bool on[4];
             unsigned long long key[4], ga[4], gb[4];
             unsigned long long *ka[4], *kb[4];
+            bool row[4];  // warp-uniform: this warp's row of the dense list holds a survivor
 #pragma unroll
             for (int q = 0; q < 4; q++) {
+                row[q] = i0 + q * kBlock + warp * 32 < total;
                 const uint32_t i = i0 + q * kBlock + threadIdx.x;
-                on[q] = i < total;
+                on[q] = row[q] && i < total;
+                ka[q] = kb[q] = nullptr;
+                ga[q] = gb[q] = 0ull;
+                rec[q] = make_uint4(0, 0, 0, 0);
+                key[q] = 0ull;
+                if (!row[q])
+                    continue;  // sparse input passes leave most rows empty
                 rec[q] = on[q] ? staging[i] : make_uint4(0, 0, 0, 0);
                 key[q] = ((unsigned long long)rec[q].z << 32) | rec[q].w;
                 const int sa = cached && on[q] ? offer_slot(s_tag, rec[q].x) : -1;
@@ -562,8 +570,8 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
             }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                if (i0 + q * kBlock + warp * 32 >= total)
-                    continue;  // warp-uniform: no survivor in this warp's row (sparse input passes)
+                if (!row[q])
+                    continue;
                 const uint32_t i = i0 + q * kBlock + threadIdx.x;
                 if (on[q])
                     out[i < split ? base + i : base2 + (i - split)] = rec[q];
