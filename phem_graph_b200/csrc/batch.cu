@@ -152,7 +152,7 @@ __device__ __forceinline__ uint32_t g_find(uint32_t *parent, uint32_t x, uint32_
 // them; older records walk with g_find.  Returns the survivor count;
 // *len_out gets the new list length.
 template <int B, int I, bool FIRST>
-__device__ uint32_t relabel_pass(const phem_edge *e0, const unsigned long long *p0, uint4 *wl, uint32_t len,
+__device__ __forceinline__ uint32_t relabel_pass(const phem_edge *e0, const unsigned long long *p0, uint4 *wl, uint32_t len,
                                  bool compact, bool fresh, uint32_t n, uint32_t kind, uint32_t *parent,
                                  unsigned long long *best, BatchSmem<B> &sm, uint32_t *len_out)
 {
@@ -230,8 +230,13 @@ struct GraphState {
     uint32_t *parent, *aux, *roots;
 };
 
-template <int B, int I>
-__device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B> &sm, unsigned char *dyn)
+// SMEM: the vertex state lives in the CTA's dynamic shared memory (graphs of
+// at most smem_vertices vertices), else in the graph's global region.  The
+// two are separate instantiations, inlined into the kernel, so every state
+// access is a plain shared- or global-memory access, never a generic one.
+template <int B, int I, bool SMEM>
+__device__ __forceinline__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B> &sm,
+                                            unsigned char *dyn)
 {
     const uint32_t n = it.n, m = it.m;
     const phem_edge *e0 = a.edges + it.e_off;
@@ -239,7 +244,7 @@ __device__ void solve_graph(const BatchArgs &a, const BatchItem &it, BatchSmem<B
     uint4 *wl = a.wl + it.wl_off;
     uint32_t *bm = a.bitmap + it.bm_off;
     GraphState g;
-    if (n <= a.smem_vertices) {
+    if (SMEM) {
         const size_t S = a.smem_vertices;
         g.best = reinterpret_cast<unsigned long long *>(dyn);
         g.parent = reinterpret_cast<uint32_t *>(dyn + 8 * S);
@@ -402,7 +407,10 @@ __global__ void __launch_bounds__(B) batch_kernel(BatchArgs a)
         if (q >= G)
             break;
         const BatchItem it = a.items[q];
-        solve_graph<B, I>(a, it, sm, dyn);
+        if (it.n <= a.smem_vertices)
+            solve_graph<B, I, true>(a, it, sm, dyn);
+        else
+            solve_graph<B, I, false>(a, it, sm, dyn);
         __syncthreads();  // sm.item, sm.err and the shared state are free again
     }
 }
