@@ -129,6 +129,23 @@ def test_out_of_range_endpoint_rejected(ctx):
     assert ctx.msf_solve(np.array([[0, 1, 1]], np.uint32), 2).count == 1
 
 
+@pytest.mark.parametrize("weight", [1, (1 << 20) + 7])
+def test_out_of_range_endpoint_rejected_filtered(ctx, weight):
+    """With the light/heavy filter on, an out-of-range endpoint is reported
+    whether its edge is light (checked by the light pass) or heavy (checked
+    by the heavy pass), and the context stays usable."""
+    g = gen.rmat_graph(14, 16, seed=4)
+    E = g.msf_edges().copy()
+    E[len(E) // 2] = (3, g.n + 5, weight)
+    with pytest.raises(P.PhemError) as ei:
+        ctx.msf_solve(E, g.n)
+    assert ei.value.status == _lib.PHEM_ERR_INVALID
+    r = ctx.msf_solve(g.msf_edges(), g.n)
+    ids, cnt, tot = expect(g.msf_edges(), g.n)
+    assert_msf(r, g.msf_edges(), ids, cnt, tot)
+    assert r.threshold != 2**64 - 1  # the filter was on
+
+
 def test_device_resident(ctx):
     import torch
     g = gen.rmat_graph(14, 16, seed=7)
