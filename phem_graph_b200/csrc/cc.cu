@@ -259,10 +259,17 @@ __device__ __forceinline__ uint32_t plain_root(const uint32_t *parent, uint32_t 
 __global__ void __launch_bounds__(kBlock) minid_scatter_kernel(int32_t n, const uint32_t *parent, uint32_t *minid,
                                                                uint32_t *err)
 {
+    // Lanes of a warp hold consecutive vertices, so among the lanes that share
+    // a root the lowest lane has the smallest id: only it reads the guard
+    // (through L1: a stale value is never below the true minimum) and
+    // offers.  A giant component's vertices no longer all hit one word.
     const int32_t stride = gridDim.x * blockDim.x;
-    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t r = plain_root(parent, (uint32_t)i, (uint32_t)n, err);
-        if ((uint32_t)i < __ldcg(minid + r))
+    for (int32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const int32_t i = i0 + (int32_t)threadIdx.x;
+        const bool in = i < n;
+        const uint32_t r = in ? plain_root(parent, (uint32_t)i, (uint32_t)n, err) : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, r);
+        if (in && (int)lane_id() == __ffs(peers) - 1 && (uint32_t)i < __ldca(minid + r))
             atomicMin(minid + r, (uint32_t)i);
     }
 }
@@ -279,13 +286,35 @@ __global__ void __launch_bounds__(kBlock) minid_label_kernel(int32_t n, const ui
 __global__ void __launch_bounds__(kBlock) cc_count_kernel(int32_t n, const int32_t *label,
                                                           const unsigned long long *forest, Ctl *ctl)
 {
+    // per-thread counts, then one atomic per warp and counter: every warp
+    // adding to the same two words once per 32 vertices serialised on them
+    __shared__ unsigned long long s_cnt[2];
+    if (threadIdx.x < 2)
+        s_cnt[threadIdx.x] = 0;
+    __syncthreads();
     const int32_t stride = gridDim.x * blockDim.x;
-    int32_t i0 = blockIdx.x * blockDim.x;
-    for (; i0 < n; i0 += stride) {
-        const int32_t i = i0 + threadIdx.x;
-        const bool in = i < n;
-        warp_count(&ctl->misc[0], in && label[i] == i);
-        warp_count(&ctl->misc[1], in && forest && forest[i] != kForestEmpty);
+    uint32_t roots = 0, slots = 0;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        roots += label[i] == i;
+        slots += forest && forest[i] != kForestEmpty;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        roots += __shfl_xor_sync(0xffffffffu, roots, d);
+        slots += __shfl_xor_sync(0xffffffffu, slots, d);
+    }
+    if (lane_id() == 0) {
+        if (roots)
+            atomicAdd(&s_cnt[0], (unsigned long long)roots);
+        if (slots)
+            atomicAdd(&s_cnt[1], (unsigned long long)slots);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_cnt[0])
+            atomicAdd(&ctl->misc[0], s_cnt[0]);
+        if (s_cnt[1])
+            atomicAdd(&ctl->misc[1], s_cnt[1]);
     }
 }
 

@@ -107,13 +107,6 @@ __device__ __forceinline__ void warp_min_to(unsigned long long *best, uint32_t t
     }
 }
 
-// Warp-aggregated counter increment; returns nothing.
-__device__ __forceinline__ void warp_count(unsigned long long *ctr, bool pred)
-{
-    const unsigned b = __ballot_sync(0xffffffffu, pred);
-    if (lane_id() == 0 && b)
-        atomicAdd(ctr, (unsigned long long)__popc(b));
-}
 
 // ---------------------------------------------------------------- block scan
 // Exclusive scan of one uint32 per thread over a kBlock-thread block.
