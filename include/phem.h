@@ -116,6 +116,9 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
  *   "msf.next_batch"        rounds queued per later check                 [4]
  *   "msf.edge_items"        records per thread in the edge pass, 4 or 8   [8]
+ *   "msf.cache_components"  list rounds that follow a round in which at most
+ *                           this many components chose an edge pre-reduce
+ *                           their offers in per-CTA shared memory     [262144]
  *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
  *                           (a prefix of the list), compresses, then the
  *                           rest; 0 unites all at once                     [1]

@@ -48,6 +48,7 @@ struct phem_context {
     uint32_t kernels_ready = 0;        // bit k: launch attributes of edge kind k are set
     int gather_blocks = 0;
     int tune_edge_items = 8;             // records per thread in the MSF edge pass (4 or 8)
+    double tune_cache_components = 262144; // MSF list rounds cache offers per CTA up to this many components
     // tuning knobs (phem_context_set_tuning)
     double tune_light_per_vertex = 0.5;  // light edges per vertex in the MSF filter (0: no filter)
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges

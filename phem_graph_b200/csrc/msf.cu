@@ -62,6 +62,7 @@ struct RoundArgs {
     uint64_t *status;
     unsigned long long *forest;
     Ctl *ctl;
+    uint64_t cache_max;  // list rounds after at most this many choosing components cache offers per CTA
 };
 
 // An input record takes part in the forest: self-loops never do; packed CC
@@ -120,7 +121,6 @@ __device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, 
 // relabel gathers rely on.
 constexpr int kOfferSlots = 1024;  // tags: 4 KB in stage 0; keys: 512 in stage 1, 512 in stage 2
 constexpr uint32_t kNoTag = 0xffffffffu;
-constexpr unsigned long long kCacheMaxComponents = 1ull << 18;
 
 // Slot of t, claiming it when free; -1 when another root holds it.
 __device__ __forceinline__ int offer_slot(uint32_t *tags, uint32_t t)
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
         reinterpret_cast<unsigned long long *>(stage_mem + 2 * stage_bytes<ITEMS>() + kFreeRow);
     auto slot_key = [&](int i) { return i < kOfferSlots / 2 ? s_key0 + i : s_key1 + (i - kOfferSlots / 2); };
     // list rounds with few components (those that chose an edge last round)
-    const bool cached = src == kSrcList && r > 0 && ctl->n_r[r - 1] <= kCacheMaxComponents;
+    const bool cached = src == kSrcList && r > 0 && ctl->n_r[r - 1] <= a.cache_max;
     if (cached)
         for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
             s_tag[i] = kNoTag;
@@ -942,6 +942,7 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.m = p.m;
     a.n = p.n;
     a.epoch_base = (uint32_t)p.epoch_base;
+    a.cache_max = (uint64_t)ctx->tune_cache_components;
     a.parent = p.parent;
     a.best = p.best;
     a.cand0 = p.cand[0];
