@@ -252,6 +252,22 @@ def test_repeated_solves_share_context(ctx):
         assert_msf(ctx.msf_solve(E, g.n), E, ids, cnt, tot)
 
 
+@pytest.mark.parametrize("cache", [0, 1024, 262144])
+def test_offer_cache_setting_does_not_change_the_forest(ctx, cache):
+    """List rounds with and without the per-CTA offer cache give the same
+    forest (hub-heavy R-MAT graph, so the cached rounds do run)."""
+    g = gen.rmat_graph(15, 16, seed=12)
+    E = g.msf_edges()
+    ids, cnt, tot = expect(E, g.n)
+    old = ctx.get_tuning("msf.cache_components")
+    ctx.set_tuning("msf.cache_components", cache)
+    try:
+        r = ctx.msf_solve(E, g.n)
+    finally:
+        ctx.set_tuning("msf.cache_components", old)
+    assert_msf(r, E, ids, cnt, tot)
+
+
 @pytest.mark.parametrize("items", [4, 8])
 def test_edge_items_variants(ctx, items):
     """Both edge-pass instantiations (4 and 8 records per thread) give the same
