@@ -584,13 +584,15 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
                 }
             }
         }
-        // this thread's staging writes and reads of the stage come before the
-        // bulk copy that will refill it
+        // This thread's staging writes and reads of the stage come before the
+        // bulk copy that will refill it.  No barrier here: the next tile's
+        // opening barrier already orders this tile's reads of staging, s_cnt
+        // and the bases before anything rewrites them (the refill of this
+        // stage is issued after the next tile's second barrier).
         fence_proxy_async_smem();
-        __syncthreads();  // staging, s_cnt and the bases are free again
     }
+    __syncthreads();  // the last tile's readers are done with the bases
     if (cached) {  // flush the shared-memory slots to best[]
-        __syncthreads();
         for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
             const uint32_t tag = s_tag[i];
             if (tag != kNoTag) {
