@@ -125,14 +125,18 @@ struct BatchSmem {
 
 // Root of x by path halving over the graph's parent array (shared or global
 // memory), bounded by n + 1 steps.  Concurrent halving writes point vertices
-// at ancestors, so walks that overlap them stay correct.
+// at ancestors, so walks that overlap them stay correct.  Plain loads: only
+// this CTA writes its graph's parent array, and it does so with plain stores
+// from this SM, so even a load served by L1 sees every write that its
+// barriers order before it (and a value missing a concurrent halving write
+// is still an ancestor).
 __device__ __forceinline__ uint32_t g_find(uint32_t *parent, uint32_t x, uint32_t n, uint32_t *err)
 {
     for (uint32_t steps = 0; steps <= n; steps++) {
-        const uint32_t p = *(volatile uint32_t *)(parent + x);
+        const uint32_t p = parent[x];
         if (p == x)
             return x;
-        const uint32_t gp = *(volatile uint32_t *)(parent + p);
+        const uint32_t gp = parent[p];
         if (gp == p)
             return p;
         parent[x] = gp;
@@ -186,8 +190,8 @@ __device__ __forceinline__ uint32_t relabel_pass(const phem_edge *e0, const unsi
             for (int j = 0; j < I; j++)
                 if (base + j * B + threadIdx.x < len) {
                     if (fresh) {
-                        rec[j].x = *(volatile uint32_t *)(parent + rec[j].x);
-                        rec[j].y = *(volatile uint32_t *)(parent + rec[j].y);
+                        rec[j].x = parent[rec[j].x];
+                        rec[j].y = parent[rec[j].y];
                     } else {
                         rec[j].x = g_find(parent, rec[j].x, n, &sm.err);
                         rec[j].y = g_find(parent, rec[j].y, n, &sm.err);
