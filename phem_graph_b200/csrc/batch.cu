@@ -90,7 +90,7 @@ __device__ __forceinline__ unsigned long long graph_key(uint32_t kind, uint32_t 
 
 __device__ __forceinline__ void offer(unsigned long long *best, uint32_t t, unsigned long long key)
 {
-    if (key < *(volatile unsigned long long *)(best + t))
+    if (key < best[t])  // a stale (higher) value only lets a redundant atomic through
         atomicMin(best + t, key);
 }
 
