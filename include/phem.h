@@ -326,7 +326,11 @@ typedef struct phem_batch_stats {
  *                               [vertex_offset, + msf_count[g]) (may be NULL);
  *   msf_count[num_graphs], msf_total[num_graphs] (required);
  *   labels[total_vertices]   <- local min-id labels (may be NULL).
- * Outputs may be host or device memory.  stats may be NULL. */
+ * Outputs may be host or device memory.  stats may be NULL.
+ * Host edges of a large batch (2^22 edges or more) are copied in four chunks
+ * on a second stream; the graphs complete after each chunk are solved by
+ * their own launch, which waits only for that chunk, so copies and solves
+ * overlap (stats->device_ms then includes the copy). */
 phem_status phem_batch_solve(phem_context *ctx, const phem_batch_graph *graphs, uint32_t num_graphs,
                              const phem_edge *edges, uint64_t total_edges, uint32_t total_vertices,
                              uint32_t *msf_ids, uint32_t *msf_count, uint64_t *msf_total, int32_t *labels,

@@ -68,6 +68,19 @@ struct BatchBuffers {
     uint32_t *status, *rounds;
 };
 
+// A large batch whose edges are in host memory is copied in kBatchGroups
+// chunks on the copy stream; the graphs whose edges are complete after chunk
+// k form launch k, which waits only for that chunk's copy, so the copies and
+// the solves overlap.
+constexpr int kBatchGroups = 4;
+constexpr uint64_t kBatchOverlapMinEdges = 1ull << 22;
+struct BatchGroups {
+    int k = 0;                           // launches; 0: one launch after one copy
+    uint64_t bound[kBatchGroups + 1];    // edge chunk boundaries
+    uint32_t start[kBatchGroups] = {};   // first item of each launch (queue order)
+    uint32_t count[kBatchGroups] = {};   // items of each launch
+};
+
 // Validated work items in queue order (largest graphs first, so the longest
 // solves start early and the persistent grid finishes together), with the
 // private scratch offsets of every graph.

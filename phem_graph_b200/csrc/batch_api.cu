@@ -89,7 +89,9 @@ size_t batch_carve(uint32_t G, uint64_t E, uint64_t wl, uint64_t bm, uint32_t V,
 {
     Carve c;
     const uint32_t g1 = G ? G : 1, v1 = V ? V : 1;
-    const size_t o_items = c.take<BatchItem>(g1), o_ng = c.take<uint32_t>(1), o_q = c.take<uint32_t>(1);
+    // num_graphs: the batch size, then the sizes of an overlapped batch's launches
+    const size_t o_items = c.take<BatchItem>(g1), o_ng = c.take<uint32_t>(1 + kBatchGroups),
+                 o_q = c.take<uint32_t>(1);
     const size_t o_e = edges_inline ? c.take<phem_edge>(E ? E : 1) : 0;
     const size_t o_wl = c.take<uint4>(wl ? wl : 1), o_bm = c.take<uint32_t>(bm ? bm : 1);
     const size_t o_gp = c.take<uint32_t>(v1), o_gc = c.take<uint32_t>(v1), o_gr = c.take<uint32_t>(v1);
@@ -151,9 +153,14 @@ phem_status batch_status(const uint32_t *status, uint32_t G)
     return ctl_status(err, "batch");
 }
 
-// Stages a batch into the context workspace: items, batch size, edges.
+// Stages a batch into the context workspace: items, batch size, edges.  With
+// `grp`, a large batch of host edges is instead grouped for overlapped
+// launches (grp->k > 0): the items are reordered by the chunk that completes
+// each graph's edges (queue order kept within a group) and the edges are
+// left for launch_overlapped to copy.
 phem_status batch_stage(phem_context *ctx, const phem_batch_graph *graphs, uint32_t G, const phem_edge *edges,
-                        uint64_t E, uint32_t V, BatchLayout *L, BatchBuffers *b, const phem_edge **d_edges)
+                        uint64_t E, uint32_t V, BatchLayout *L, BatchBuffers *b, const phem_edge **d_edges,
+                        BatchGroups *grp = nullptr)
 {
     PHEM_TRY(build_items(graphs, G, E, V, L));
     if (E && !edges) {
@@ -164,14 +171,38 @@ phem_status batch_stage(phem_context *ctx, const phem_batch_graph *graphs, uint3
     const size_t bytes = batch_carve(G, E, L->wl_records, L->bm_words, V, !dev_edges, nullptr, nullptr);
     PHEM_TRY(ws_reserve(ctx, bytes));
     batch_carve(G, E, L->wl_records, L->bm_words, V, !dev_edges, static_cast<char *>(ctx->ws), b);
+    uint32_t nums[1 + kBatchGroups] = {G};
+    if (grp && !dev_edges && E >= kBatchOverlapMinEdges && G >= 2) {
+        grp->k = kBatchGroups;
+        for (int k = 0; k <= kBatchGroups; k++)
+            grp->bound[k] = E * (uint64_t)k / kBatchGroups;
+        std::vector<BatchItem> by_group;
+        by_group.reserve(G);
+        for (int k = 0; k < kBatchGroups; k++) {
+            grp->start[k] = (uint32_t)by_group.size();
+            for (const BatchItem &it : L->items) {
+                const uint64_t end = it.e_off + it.m;
+                int g = 0;
+                while (g + 1 < kBatchGroups && end > grp->bound[g + 1])
+                    g++;
+                if (g == k)
+                    by_group.push_back(it);
+            }
+            grp->count[k] = (uint32_t)by_group.size() - grp->start[k];
+            nums[1 + k] = grp->count[k];
+        }
+        L->items.swap(by_group);
+    } else if (grp) {
+        grp->k = 0;
+    }
     if (G)
         PHEM_CUDA_TRY(cudaMemcpyAsync(b->items, L->items.data(), sizeof(BatchItem) * G, cudaMemcpyHostToDevice,
                                       ctx->stream));
-    PHEM_CUDA_TRY(cudaMemcpyAsync(b->num_graphs, &G, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    PHEM_CUDA_TRY(cudaMemcpyAsync(b->num_graphs, nums, sizeof(nums), cudaMemcpyHostToDevice, ctx->stream));
     if (dev_edges) {
         *d_edges = edges;
     } else {
-        if (E)
+        if (E && !(grp && grp->k))
             PHEM_CUDA_TRY(cudaMemcpyAsync(b->edges, edges, sizeof(phem_edge) * E, cudaMemcpyDefault, ctx->stream));
         *d_edges = b->edges;
     }
@@ -185,6 +216,54 @@ phem_status launch_once(phem_context *ctx, const BatchLaunch &l, const BatchArgs
     PHEM_CUDA_TRY(cudaMemsetAsync(args.queue, 0, sizeof(uint32_t), ctx->stream));
     KernelScope k(ctx, kKBatch);
     return batch_launch(ctx->stream, l, args);
+}
+
+// The launches of an overlapped batch: chunk k of the host edges is copied on
+// the copy stream, and launch k (the graphs complete after chunk k) waits
+// only for it.
+phem_status launch_overlapped(phem_context *ctx, const BatchLaunch &l, const BatchArgs &args,
+                              const BatchGroups &grp, const phem_edge *h_edges, phem_edge *d_edges,
+                              const BatchBuffers &b)
+{
+    cudaEvent_t ev[kBatchGroups + 1] = {};
+    phem_status st = PHEM_OK;
+    for (auto &e : ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            e = nullptr;
+            set_error("batch: cannot create copy events");
+            st = PHEM_ERR_CUDA;
+        }
+    // the first copy waits for earlier work on the context stream, which may
+    // still read the workspace
+    if (st == PHEM_OK && (cudaEventRecord(ev[kBatchGroups], ctx->stream) != cudaSuccess ||
+                          cudaStreamWaitEvent(ctx->copy_stream, ev[kBatchGroups], 0) != cudaSuccess)) {
+        set_error("batch: cannot order the copy stream");
+        st = PHEM_ERR_CUDA;
+    }
+    for (int k = 0; st == PHEM_OK && k < grp.k; k++) {
+        const uint64_t lo = grp.bound[k], cnt = grp.bound[k + 1] - lo;
+        if ((cnt && cudaMemcpyAsync(d_edges + lo, h_edges + lo, sizeof(phem_edge) * cnt, cudaMemcpyDefault,
+                                    ctx->copy_stream) != cudaSuccess) ||
+            cudaEventRecord(ev[k], ctx->copy_stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ctx->stream, ev[k], 0) != cudaSuccess) {
+            set_error("batch: chunk copy failed: %s", cudaGetErrorString(cudaGetLastError()));
+            st = PHEM_ERR_CUDA;
+            break;
+        }
+        if (grp.count[k]) {
+            BatchArgs a = args;
+            a.items = args.items + grp.start[k];
+            a.num_graphs = b.num_graphs + 1 + k;
+            st = launch_once(ctx, l, a);
+        }
+    }
+    if (st != PHEM_OK)
+        cudaStreamSynchronize(ctx->copy_stream);  // no copy may still land in the workspace
+    for (auto e : ev)
+        if (e)
+            cudaEventDestroy(e);
+    return st;
 }
 
 void fill_stats(phem_batch_stats *st, const BatchLaunch &l, float ratio, float ms, uint32_t max_rounds)
@@ -265,7 +344,8 @@ phem_status phem_batch_solve(phem_context *ctx, const phem_batch_graph *graphs, 
     BatchLayout L;
     BatchBuffers b{};
     const phem_edge *d_edges = nullptr;
-    PHEM_TRY(batch_stage(ctx, graphs, num_graphs, edges, total_edges, total_vertices, &L, &b, &d_edges));
+    BatchGroups grp;
+    PHEM_TRY(batch_stage(ctx, graphs, num_graphs, edges, total_edges, total_vertices, &L, &b, &d_edges, &grp));
     BatchLaunch l;
     PHEM_TRY(batch_launch_config(ctx->device, ctx->sm_count, ctx->tune_batch_block, ctx->tune_batch_items, &l));
     const float ratio = (float)ctx->tune_batch_compact;
@@ -273,7 +353,10 @@ phem_status phem_batch_solve(phem_context *ctx, const phem_batch_graph *graphs, 
     float ms = 0.f;
     {
         Timed timer(ctx);
-        PHEM_TRY(launch_once(ctx, l, args));
+        if (grp.k)
+            PHEM_TRY(launch_overlapped(ctx, l, args, grp, edges, b.edges, b));
+        else
+            PHEM_TRY(launch_once(ctx, l, args));
         ms = timer.stop();
     }
     PHEM_CUDA_TRY(cudaGetLastError());

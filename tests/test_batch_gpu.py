@@ -158,6 +158,26 @@ def test_plan_replay_two_batches(ctx):
         assert all(v for v in p.device().values())
 
 
+def test_large_host_batch_overlapped_launches(ctx):
+    """A batch of host edges past the overlap size is copied in chunks and
+    solved by one launch per chunk group (graphs straddling chunk ends go
+    to the later group); every graph's forest, count, total and labels equal
+    the single-launch result of a plan, twice in a row."""
+    b = gen.mixed_batch(160, 21, n_lo=64, n_hi=65536, threads=8)
+    assert b.total_edges >= 1 << 22
+    with ctx.batch_plan(b.num_graphs, b.total_edges, b.total_vertices) as p:
+        p.upload(b)
+        p.run()
+        want = p.download(labels=True)
+    for _ in range(2):
+        got = ctx.batch_solve(b)
+        np.testing.assert_array_equal(got.count, want.count)
+        np.testing.assert_array_equal(got.total, want.total)
+        np.testing.assert_array_equal(got.labels, want.labels)
+        for g in range(b.num_graphs):
+            np.testing.assert_array_equal(got.forest(b, g), want.forest(b, g))
+
+
 def test_plan_rejects_oversized_batch(ctx):
     a = small_mixed(8, seed=4)
     with ctx.batch_plan(4, a.total_edges, a.total_vertices) as p:
