@@ -56,7 +56,11 @@ def main() -> None:
         print("cc no-alloc ok")
 
         b = gen.mixed_batch(256, 4)
-        print("batch", ctx.batch_solve(b, labels=False).stats)
+        with ctx.batch_plan(b.num_graphs, b.total_edges, b.total_vertices) as plan:
+            plan.upload(b)  # device-resident edges: one launch, no overlapped copies
+            plan.run()
+            r = plan.download(labels=False)
+        print("batch", b.num_graphs, "graphs ->", int(r.count.sum()), "forest edges")
         torch.cuda.synchronize()
 
 
