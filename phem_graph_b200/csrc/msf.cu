@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
     __shared__ uint64_t s_bar[kStages];
     __shared__ uint32_t s_cnt[kCnt];
     __shared__ unsigned long long s_base, s_base2;
-    __shared__ uint32_t s_split, s_total;
+    __shared__ uint32_t s_split;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
@@ -480,67 +480,67 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
                                    &s_bar[s2], stream_policy);
             }
         }
-        if (warp == 0) {
-            // exclusive scan of the row/warp counts, row-major, kCnt / 32 per lane
-            constexpr int kPer = kCnt / 32;
-            uint32_t c[kPer], sum = 0;
+        // Every warp scans the row/warp counts (row-major, kCnt / 32 per lane)
+        // itself, so the ranks need no barrier of their own; warp 0 also
+        // reserves the tile's output range, which the staging barrier below
+        // publishes before the dense phase reads it.
+        constexpr int kPer = kCnt / 32;
+        static_assert(kPer == 1 || kPer == 2, "row/warp counts per lane");
+        uint32_t c[kPer], sum = 0;
 #pragma unroll
-            for (int q = 0; q < kPer; q++) {
-                c[q] = s_cnt[kPer * lane + q];
-                sum += c[q];
-            }
-            uint32_t incl = sum;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= (uint32_t)d)
-                    incl += y;
-            }
-            uint32_t run = incl - sum;
-#pragma unroll
-            for (int q = 0; q < kPer; q++) {
-                s_cnt[kPer * lane + q] = run;
-                run += c[q];
-            }
-            if (lane == 31) {
-                const unsigned long long total = incl;
-                s_total = (uint32_t)total;
-                s_base = chunk_next;
-                if (total <= chunk_left) {
-                    s_split = (uint32_t)total;
-                    chunk_next += total;
-                    chunk_left -= total;
-                } else {
-                    // the first chunk_left survivors finish the current chunk, the
-                    // rest open a new one sized to this CTA's remaining input
-                    s_split = (uint32_t)chunk_left;
-                    const unsigned long long rest = total - chunk_left;
-                    const uint64_t tiles_left = (ntiles - 1 - t) / gridDim.x + 1;
-                    const unsigned long long cap = tiles_left * tile_recs;
-                    const unsigned long long want = cap < kChunk ? cap : kChunk;
-                    const unsigned long long size = want > rest ? want : rest;
-                    const unsigned long long fresh = atomicAdd(&ctl->wl_len[r], size);
-                    s_base2 = fresh;
-                    chunk_next = fresh + rest;
-                    chunk_left = size - rest;
-                }
-                live += total;
-            }
+        for (int q = 0; q < kPer; q++) {
+            c[q] = s_cnt[kPer * lane + q];
+            sum += c[q];
         }
-        __syncthreads();  // ranks, bases and split are ready
+        uint32_t incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (uint32_t)d)
+                incl += y;
+        }
+        const uint32_t ex0 = incl - sum, ex1 = ex0 + c[0];
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        if (warp == 0 && lane == 31) {
+            s_base = chunk_next;
+            if (total <= chunk_left) {
+                s_split = total;
+                chunk_next += total;
+                chunk_left -= total;
+            } else {
+                // the first chunk_left survivors finish the current chunk, the
+                // rest open a new one sized to this CTA's remaining input
+                s_split = (uint32_t)chunk_left;
+                const unsigned long long rest = total - chunk_left;
+                const uint64_t tiles_left = (ntiles - 1 - t) / gridDim.x + 1;
+                const unsigned long long cap = tiles_left * tile_recs;
+                const unsigned long long want = cap < kChunk ? cap : kChunk;
+                const unsigned long long size = want > rest ? want : rest;
+                const unsigned long long fresh = atomicAdd(&ctl->wl_len[r], size);
+                s_base2 = fresh;
+                chunk_next = fresh + rest;
+                chunk_left = size - rest;
+            }
+            live += total;
+        }
         // Stage the survivors densely, in rank (= input) order, in this
         // tile's own stage buffer: its input is already in registers, and the
-        // buffer is refilled only after this tile's last barrier.
+        // buffer is refilled only after the next tile's second barrier.
         uint4 *staging = reinterpret_cast<uint4 *>(stage);
         const unsigned below = (1u << lane) - 1u;
 #pragma unroll
-        for (int j = 0; j < ITEMS; j++)
+        for (int j = 0; j < ITEMS; j++) {
+            // exclusive offset of entry (row j, this warp): lane e / kPer holds it
+            const uint32_t e = j * kWarps + warp;
+            const uint32_t mine = (kPer == 2 && (e & 1)) ? ex1 : ex0;
+            const uint32_t off = __shfl_sync(0xffffffffu, mine, e / kPer);
             if (mask[j] && keep[j])  // mask: warp-uniform skip of rows without survivors
-                staging[s_cnt[j * kWarps + warp] + __popc(mask[j] & below)] = make_uint4(ra[j], rb[j], w[j], id[j]);
-        __syncthreads();
+                staging[off + __popc(mask[j] & below)] = make_uint4(ra[j], rb[j], w[j], id[j]);
+        }
+        __syncthreads();  // staging, bases and split are ready
         // Dense phase: coalesced survivor writes and the offers of both
         // endpoints, several records per thread so the guard loads overlap.
-        const uint32_t total = s_total, split = s_split;
+        const uint32_t split = s_split;
         const unsigned long long base = s_base, base2 = s_base2;
         for (uint32_t i0 = 0; i0 < total; i0 += kBlock * 4) {
             uint4 rec[4];
