@@ -119,6 +119,8 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.cache_components"  list rounds that follow a round in which at most
  *                           this many components chose an edge pre-reduce
  *                           their offers in per-CTA shared memory     [262144]
+ *   "cc.canonical_light_per_vertex"  msf.light_per_vertex for the
+ *                           PHEM_CC_CANONICAL forest (light = first by index) [2]
  *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
  *                           (a prefix of the list), compresses, then the
  *                           rest; 0 unites all at once                     [1]

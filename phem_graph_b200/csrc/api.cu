@@ -418,6 +418,8 @@ phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double v
         ctx->tune_next_batch = (int)value;
     } else if (k == "msf.edge_items" && (value == 4 || value == 8)) {
         ctx->tune_edge_items = (int)value;
+    } else if (k == "cc.canonical_light_per_vertex" && value >= 0 && value < 1e6) {
+        ctx->tune_canonical_light = value;
     } else if (k == "msf.cache_components" && value >= 0.0 && value < 4294967296.0) {
         ctx->tune_cache_components = value;
     } else if (k == "cc.sample_per_vertex" && value >= 0.0 && value < 1e6) {
@@ -447,6 +449,8 @@ phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *
         *value = ctx->tune_light_per_vertex;
     else if (k == "msf.filter_min_ratio")
         *value = ctx->tune_filter_min_ratio;
+    else if (k == "cc.canonical_light_per_vertex")
+        *value = ctx->tune_canonical_light;
     else if (k == "msf.cache_components")
         *value = ctx->tune_cache_components;
     else if (k == "msf.first_batch")

@@ -51,6 +51,7 @@ struct phem_context {
     double tune_cache_components = 262144; // MSF list rounds cache offers per CTA up to this many components
     // tuning knobs (phem_context_set_tuning)
     double tune_light_per_vertex = 0.5;  // light edges per vertex in the MSF filter (0: no filter)
+    double tune_canonical_light = 2.0;   // the same for the canonical CC forest (edges by index)
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
     int tune_first_batch = 8;            // Boruvka rounds queued before the first host check
     int tune_next_batch = 4;             // rounds queued per later check

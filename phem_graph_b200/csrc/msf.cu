@@ -1020,7 +1020,9 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
     const RoundArgs a = make_args(ctx, plan);
     // light/heavy split: about light_per_vertex * n light edges, and only when
     // the input is at least filter_min_ratio times that large
-    const double lpv = ctx->tune_light_per_vertex;
+    // the canonical forest's light edges are the first ones by index, which
+    // start forming the large components only at about two per vertex
+    const double lpv = KIND == kKindPacked ? ctx->tune_canonical_light : ctx->tune_light_per_vertex;
     const uint64_t k = (uint64_t)(lpv * (double)plan.n);
     const bool filter = lpv > 0 && k > 0 && (double)plan.m >= ctx->tune_filter_min_ratio * (double)k;
     unsigned long long thr = kKeyNone;

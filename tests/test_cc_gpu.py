@@ -189,6 +189,23 @@ def test_stream_unsorted_rmat_batches(ctx):
     check_forest(pairs, n, got, forest.cpu().numpy().view(np.uint64))
 
 
+@pytest.mark.parametrize("light", [0.0, 0.5, 2.0, 6.0])
+def test_canonical_filter_setting_does_not_change_the_forest(ctx, light):
+    """The canonical forest's light/heavy split (first edges by index) gives
+    the sequential reference's forest set for any split size, unfiltered
+    included."""
+    g = gen.er_graph(1 << 15, 1 << 18, 23)
+    want_labels, want_forest = oracle.cc_solve(g.pairs, g.n)
+    saved = ctx.get_tuning("cc.canonical_light_per_vertex")
+    try:
+        ctx.set_tuning("cc.canonical_light_per_vertex", light)
+        rc = ctx.cc_solve(g.pairs, g.n, canonical=True)
+    finally:
+        ctx.set_tuning("cc.canonical_light_per_vertex", saved)
+    np.testing.assert_array_equal(rc.labels, want_labels)
+    np.testing.assert_array_equal(forest_set(rc.forest), oracle.forest_set(want_forest))
+
+
 @pytest.mark.parametrize("sample", [0.0, 0.5, 2.0, 1000.0])
 def test_sample_schedule_same_labels(ctx, sample):
     """The prefix-sample / compress / rest schedule gives the same labels and
