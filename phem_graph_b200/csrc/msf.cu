@@ -33,7 +33,7 @@
 // no record has to be looked up and the survivor list may be in any order.
 // That removes every dependency between CTAs from the edge pass: tiles are
 // statically strided over a persistent grid, arrive in shared memory by 1-D
-// bulk copies (cp.async.bulk) two tiles ahead of use, survivors are staged
+// bulk copies (cp.async.bulk) one tile ahead of use, survivors are staged
 // densely in shared memory before their coalesced write, and output space is
 // reserved in chunks with one atomicAdd each.  MSF membership is a bitmap over
 // edge ids; one ordered gather (decoupled look-back) writes the MSF records
@@ -115,11 +115,10 @@ __device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, 
 // A root owns a slot (t mod kOfferSlots) once it claims it; offers to owned
 // slots are shared-memory atomicMin, the rest go to best[] directly, and the
 // slots are flushed to best[] when the CTA's tiles are done.  The slots live
-// in the last row of the three stage buffers, which list rounds leave free
-// (their tiles are one row shorter): more static shared memory would push
-// two CTAs per SM past a carveout step and halve the L1 the heavy pass's
-// relabel gathers rely on.
-constexpr int kOfferSlots = 1024;  // tags: 4 KB in stage 0; keys: 512 in stage 1, 512 in stage 2
+// in the last row of the two stage buffers, which list rounds leave free
+// (their tiles are one row shorter): more shared memory would take L1 from
+// the heavy pass's relabel gathers, which depend on it.
+constexpr int kOfferSlots = 512;  // tags: 2 KB in stage 0; keys: 4 KB in stage 1
 constexpr uint32_t kNoTag = 0xffffffffu;
 
 // Slot of t, claiming it when free; -1 when another root holds it.
@@ -275,14 +274,16 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
 }
 
 // One Boruvka round's edge pass: relabel + filter + compaction + per-root
-// minimum.  Tile k of a CTA is tile blockIdx.x + k * gridDim.x; stage k % 3 of
-// shared memory receives it by bulk copy two iterations ahead.  Threads read
+// minimum.  Tile k of a CTA is tile blockIdx.x + k * gridDim.x; stage k % 2 of
+// shared memory receives it by bulk copy one iteration ahead.  Threads read
 // a tile striped (record j * kBlock + tid), conflict-free for 8, 12 and
 // 16-byte records.  Survivor ranks inside the tile come from warp ballots and
-// a scan of the (row, warp) counts; warp 0 reserves the tile's output range
-// with one atomicAdd on the round's counter while every warp is already
-// updating component slots.
-constexpr int kStages = 3;
+// a scan of the (row, warp) counts that every warp does itself; warp 0
+// reserves the tile's output range from the CTA's chunk of the list.
+// Two stages: a tile's bulk copy is issued one tile ahead, which was enough
+// to find the next tile ready on 99 % of waits with three stages; the third
+// stage's 32 KB per CTA went back to L1 (heavy pass 555 -> 526 us).
+constexpr int kStages = 2;
 constexpr unsigned long long kChunk = 4096;  // output records reserved per atomicAdd
 constexpr uint64_t kMaxEdgeCtasPerSm = 4;      // edge-pass grid bound (sizes the list padding)
 
@@ -297,8 +298,8 @@ __host__ __device__ constexpr size_t pipe_smem()
     return kStages * stage_bytes<ITEMS>();
 }
 
-// Resident CTAs per SM: two for 8 records per thread (the three stages fill
-// shared memory), three for 4 (half the stage bytes; registers capped to fit).
+// Resident CTAs per SM: two for 8 records per thread (registers), three for
+// 4 (registers capped to fit).
 template <int KIND, int ITEMS>
 __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(RoundArgs a)
 {
@@ -320,9 +321,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
     constexpr size_t kFreeRow = (size_t)(ITEMS - 1) * kBlock * 16;
     uint32_t *s_tag = reinterpret_cast<uint32_t *>(stage_mem + kFreeRow);
     unsigned long long *s_key0 = reinterpret_cast<unsigned long long *>(stage_mem + stage_bytes<ITEMS>() + kFreeRow);
-    unsigned long long *s_key1 =
-        reinterpret_cast<unsigned long long *>(stage_mem + 2 * stage_bytes<ITEMS>() + kFreeRow);
-    auto slot_key = [&](int i) { return i < kOfferSlots / 2 ? s_key0 + i : s_key1 + (i - kOfferSlots / 2); };
+    auto slot_key = [&](int i) { return s_key0 + i; };
     // list rounds with few components (those that chose an edge last round)
     const bool cached = src == kSrcList && r > 0 && ctl->n_r[r - 1] <= a.cache_max;
     if (cached)
@@ -470,7 +469,7 @@ __global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(R
                 s_cnt[j * kWarps + warp] = __popc(mask[j]);
         __syncthreads();  // s_cnt complete; every record of the stage is in registers
         if (threadIdx.x == 0) {
-            // refill the stage read last iteration with the tile two ahead
+            // refill the stage read last iteration with the next tile of this CTA
             const uint64_t t2 = t + (uint64_t)(kStages - 1) * gridDim.x;
             const int s2 = (s + kStages - 1) % kStages;
             if (t2 < full_tiles) {
