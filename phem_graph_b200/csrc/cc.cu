@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kBlock) cc_label_kernel(int32_t n, int32_t *pa
 {
     const int32_t stride = gridDim.x * blockDim.x;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const int32_t r = uf_find<false>(parent, i, n, err);
+        const int32_t r = uf_find<true>(parent, i, n, err);
         label[i] = r;
         if (parent[i] != r)
             parent[i] = r;
@@ -233,12 +233,15 @@ __global__ void __launch_bounds__(kBlock) cc_label_kernel(int32_t n, int32_t *pa
 }
 
 // parent[i] = root(i) for every vertex (no labels): after it every later
-// union's first two loads already compare roots.
+// union's first two loads already compare roots.  Here and in the label pass
+// the walks read through L1: no union runs, so roots are final, L1 starts
+// each launch without lines of earlier launches, and a value that misses a
+// concurrent halving write is still an ancestor.
 __global__ void __launch_bounds__(kBlock) cc_compress_kernel(int32_t n, int32_t *parent, uint32_t *err)
 {
     const int32_t stride = gridDim.x * blockDim.x;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const int32_t r = uf_find<false>(parent, i, n, err);
+        const int32_t r = uf_find<true>(parent, i, n, err);
         if (parent[i] != r)
             parent[i] = r;
     }
