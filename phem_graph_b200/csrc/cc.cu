@@ -14,7 +14,8 @@
 //   * a union first compares the endpoints' parents (two loads settle most
 //     edges once trees are flat), then walks both roots in lockstep so the
 //     two walks' loads overlap, stopping early where the walks meet; the
-//     first walk reads through L1, a walk after a failed CAS through L2;
+//     first walk reads through L1, a walk after a failed CAS through L2,
+//     continuing from the parent the CAS returned;
 //   * path halving writes are atomic mins: ids fall towards the root, so a
 //     walk working from a stale parent never undoes another walk's shortcut;
 //   * phem_cc_solve unites a prefix of about one edge per vertex, points
@@ -147,13 +148,16 @@ __device__ __forceinline__ bool uf_unite(int32_t *parent, unsigned long long *fo
         if ((retry & 63) == 63 && (*(volatile uint32_t *)err & (kErrChase | kErrRetry)))
             return false;  // another thread already reported a broken state
         const int32_t hi = ru > rv ? ru : rv, lo = ru > rv ? rv : ru;
-        if (atomicCAS(parent + hi, hi, lo) == hi) {
+        const int32_t old = atomicCAS(parent + hi, hi, lo);
+        if (old == hi) {
             if (forest)
                 forest[hi] = e;
             return true;
         }
-        u = ru;  // both are ancestors of the original endpoints
-        v = rv;
+        // hi was hooked under `old` meanwhile: walk on from there (both are
+        // ancestors of the original endpoints)
+        u = old;
+        v = lo;
     }
     set_err(err, kErrRetry);
     return false;
