@@ -21,6 +21,8 @@ Workload (one "step" = one full minimum-spanning-forest solve):
 On one GPU the same JSON line also carries the metric's other workloads:
   csr_input  the same R-MAT solve fed as its symmetrised CSR (int64 offsets,
            uint32 columns) and per-edge weights, converted on the device;
+  msf_chunked  the same pinned host edges through phem_msf_stream (the
+           reference's chunked streamline mode), 2^24 edges per chunk;
   cc       connected components + forest, Erdos-Renyi n = 2^20, 8 * 2^20 draws;
   batched  4096 small graphs (ER and geometric) in one persistent launch,
            against one solve per graph;
@@ -476,6 +478,104 @@ def bench_streamed(ctx, torch, scale: int, edge_factor: int = 32, batch: int = 1
                        "sampled_edges_join_equal_labels": ok_edges}}
 
 
+def bench_msf_chunked(ctx, h_pinned, n: int, one_shot_s: float, expect: tuple, chunk: int = 1 << 24) -> dict:
+    """The MSF workload through phem_msf_stream (the reference's
+    streamline_boruvka): pinned host records in chunks of `chunk` edges, each
+    solved with the forest so far while the next chunk is copied; host forest
+    out.  Wall time per call, median of 3, beside the one-shot phem_msf_solve
+    of the same pinned input (the headline e2e)."""
+    m = int(h_pinned.shape[0])
+    out = np.empty((n, 3), np.uint32)
+    ctx.msf_stream(h_pinned, n, chunk, out=out)  # warm-up
+    times, dev_ms, r = [], [], None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        r = ctx.msf_stream(h_pinned, n, chunk, out=out)
+        times.append(time.perf_counter() - t0)
+        dev_ms.append(r.device_ms)
+    t = float(np.median(times))
+    return {"workload": f"msf_rmat_chunked_{m}_chunk2^{chunk.bit_length() - 1}", "n": n, "m": m, "unit": UNIT,
+            "chunks": -(-m // chunk), "value": m / t / 1e9, "ms_per_solve": t * 1e3,
+            "device_ms": float(np.median(dev_ms)), "one_shot_e2e_ms": one_shot_s * 1e3,
+            "result_matches_one_shot": (r.count, r.total) == expect,
+            "api": "phem_msf_stream (C ABI), pinned host edges and forest, median of 3"}
+
+
+def bench_msf_chunked_large(ctx, torch, scale: int, edge_factor: int = 16, chunk: int = 1 << 28) -> dict:
+    """Chunked MSF beyond one solve's 2^32-edge limit: R-MAT at `scale` with
+    edge_factor * 2^scale draws (seed 28, self-loops dropped, unsorted; at
+    scale 28 about 4.29 G edges, 51.5 GB of records), weights uniform in
+    [1, 2^20] from a SplitMix64 stream per 2^28 draws, generated into pinned
+    host memory before timing and streamed through phem_msf_stream.  Checked
+    by size-independent properties: a second run with a ragged chunk size
+    returns the identical forest; the forest is acyclic (connected components
+    of the forest edges alone number n - count); its weights sum to the total."""
+    import ctypes as C
+
+    from phem_graph_b200 import _lib
+    n = 1 << scale
+    draws = edge_factor << scale
+    h = torch.empty((draws, 3), dtype=torch.int32, pin_memory=True)
+    gen_chunk = 1 << 28
+    pairs = np.empty(gen_chunk, np.uint64)
+    w = np.empty(gen_chunk, np.uint32)
+    filled = 0
+    t_gen = time.perf_counter()
+    for k, first in enumerate(range(0, draws, gen_chunk)):
+        cnt = C.c_uint64()
+        want = min(gen_chunk, draws - first)
+        _lib.check(_lib.lib().phem_gen_rmat_range(scale, first, want, 0.57, 0.19, 0.19, 28, pairs.ctypes.data,
+                                                  C.byref(cnt)), "phem_gen_rmat_range")
+        c = cnt.value
+        _lib.check(_lib.lib().phem_gen_weights(c, 1000 + k, 20, w.ctypes.data), "phem_gen_weights")
+        _lib.check(_lib.lib().phem_pack_msf_edges(pairs.ctypes.data, w.ctypes.data, c,
+                                                  h.data_ptr() + 12 * filled), "phem_pack_msf_edges")
+        filled += c
+    t_gen = time.perf_counter() - t_gen
+    del pairs, w
+    m = filled
+    hv = h[:m]
+    dev = torch.device("cuda", ctx.device)
+    # host link bandwidth for the roofline: one pinned copy of a chunk
+    probe = torch.empty((min(chunk, m), 3), dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    probe.copy_(hv[: probe.shape[0]], non_blocking=True)
+    torch.cuda.synchronize()
+    h2d_gbs = 12 * probe.shape[0] / (time.perf_counter() - t0) / 1e9
+    del probe
+    torch.cuda.empty_cache()
+    out_a = torch.empty((n, 3), dtype=torch.int32, pin_memory=True)
+    out_b = torch.empty((n, 3), dtype=torch.int32, pin_memory=True)
+    t0 = time.perf_counter()
+    ra = ctx.msf_stream(hv, n, chunk, out=out_a)
+    t_a = time.perf_counter() - t0
+    ragged = chunk - (1 << 20) + 7
+    rb = ctx.msf_stream(hv, n, ragged, out=out_b)
+    same = (ra.count, ra.total) == (rb.count, rb.total) and bool(torch.equal(out_a[:ra.count], out_b[:rb.count]))
+    del out_b
+    f = out_a[:ra.count].numpy().view(np.uint32)
+    total_ok = int(f[:, 2].sum(dtype=np.uint64)) == ra.total
+    fd = torch.from_numpy(f.view(np.int32)).to(dev).long() & 0xFFFFFFFF
+    lo, hi = torch.minimum(fd[:, 0], fd[:, 1]), torch.maximum(fd[:, 0], fd[:, 1])
+    packed = (lo << 32) | hi
+    labels = torch.empty(n, dtype=torch.int32, device=dev)
+    comps = ctx.cc_solve(packed, n, labels=labels).components
+    del fd, lo, hi, packed, labels
+    torch.cuda.empty_cache()
+    return {"workload": f"msf_rmat{scale}_ef{edge_factor}_chunked_chunk2^{chunk.bit_length() - 1}", "n": n, "m": m,
+            "chunks": -(-m // chunk), "unit": UNIT, "value": m / t_a / 1e9, "ms": t_a * 1e3,
+            "device_ms": ra.device_ms, "generation_s": t_gen, "msf_edges": ra.count, "total_weight": ra.total,
+            "roofline": {"bound": "host link", "achieved": 12 * m / (ra.device_ms / 1e3) / 1e9, "peak": h2d_gbs,
+                         "unit": "GB/s", "frac": 12 * m / (ra.device_ms / 1e3) / 1e9 / h2d_gbs,
+                         "peak_source": "one pinned host-to-device copy of a chunk, measured here"},
+            "host_bytes": 12 * m,
+            "device_bytes": "2 x (n - 1 + chunk) records of input slots, n - 1 output records, one solve's workspace",
+            "api": "phem_msf_stream (C ABI), pinned host records, pinned host forest",
+            "checks": {"ragged_chunks_same_forest": same, "forest_acyclic": comps == n - ra.count,
+                       "weights_sum_to_total": total_ok}}
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's own CPU path (PBBS mst()) on the same
     workload, all host threads; one step = one full solve."""
@@ -533,6 +633,9 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--stream-scale", type=int, default=0,
                     help="also stream an R-MAT graph of this scale (edge factor 32) from pinned host memory")
+    ap.add_argument("--msf-stream-scale", type=int, default=0,
+                    help="also solve an R-MAT graph of this scale (edge factor 16) by chunked MSF from pinned "
+                         "host memory (scale 28: 4.29 G edges, beyond one solve's 2^32 limit)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the connected-components, batched and served workloads")
     args = ap.parse_args()
@@ -686,11 +789,15 @@ def main() -> None:
         torch.cuda.empty_cache()
         line["csr_input"] = bench_csr_input(ctx, torch, g, max(3, args.steps // 2), args.warmup,
                                             (stats.count, stats.total))
+        line["msf_chunked"] = bench_msf_chunked(ctx, h_pinned, n, e2e_s, (stats.count, stats.total))
         line["cc"] = bench_cc(ctx, torch, peaks, args.steps, args.warmup, not args.no_cpu_baseline)
         line["batched"] = bench_batched(ctx, torch)
         line["served"] = bench_served(torch)
     if rank == 0 and world == 1 and args.stream_scale:
         line["streamed"] = bench_streamed(ctx, torch, args.stream_scale)
+    if rank == 0 and world == 1 and args.msf_stream_scale:
+        del h_pinned, h_out
+        line["msf_chunked_large"] = bench_msf_chunked_large(ctx, torch, args.msf_stream_scale)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()

@@ -268,6 +268,22 @@ phem_status phem_msf_solve(phem_context *ctx, const phem_edge *edges, uint64_t m
 phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, uint64_t m, uint32_t n,
                                   phem_edge *d_msf, uint64_t *d_count_total, phem_msf_stats *stats);
 
+/* Chunked MSF over host-resident edges: streamline_boruvka
+ * (MST/src/kernels.cu:849-1154).  h_edges[0..m) is taken in chunks of `chunk`
+ * edges; chunk k is solved together with the forest of chunks 0..k-1
+ * (MSF(G1 + G2) = MSF(MSF(G1) + G2)), while chunk k + 1 is copied on a second
+ * stream.  The result is exactly phem_msf_solve's -- the unique MSF under
+ * (w, edge index), ascending by edge index -- but m has no 2^32 limit: each
+ * solve holds one chunk plus at most n - 1 forest edges, so device memory
+ * scales with chunk + n, not m.
+ *   msf (host or device, room for n - 1 records, may be NULL), *count, *total
+ *   as phem_msf_solve; *ms = device time from the first copy to the last solve.
+ * Needs 0 < chunk and chunk + n <= 2^32 - 2^24 (roughly).  h_edges may be host
+ * (pinned for the copies to overlap) or device memory.  count, total and ms
+ * may be NULL. */
+phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_t m, uint32_t n, uint64_t chunk,
+                            phem_edge *msf, uint64_t *count, uint64_t *total, float *ms);
+
 /* MSF of a symmetrised CSR graph (int64 offsets[n + 1], uint32 cols[2m]).
  * Edge i is the i-th entry with row < col in row-major order (the numbering of
  * csr_to_coo, CC/graph.cu:169-187); weights[i] is its weight.  Output as

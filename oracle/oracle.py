@@ -134,6 +134,26 @@ def msf_boruvka(E, n: int, max_rounds: int = 64):
     return flags[:m].astype(bool), int(cnt.value), int(tot.value), m_r[:r].copy(), n_r[:r].copy()
 
 
+def msf_chunked(E, n: int, chunk: int):
+    """Chunked MSF of streamline_boruvka (MST/src/kernels.cu:849-1154): each
+    chunk is solved together with the forest of the chunks before it
+    (kernels.cu:942-997 appends the previous MSF to the next chunk).  The
+    carried forest goes first, ascending by global edge id, so Kruskal's
+    (w, position) order is the global (w, id) order.  Returns (in_msf, count,
+    total) over the global ids."""
+    E = _edges3(E)
+    m = len(E)
+    carried = np.zeros(0, np.int64)  # global ids of the forest so far
+    count = total = 0
+    for off in range(0, m, chunk):
+        ids = np.concatenate([carried, np.arange(off, min(m, off + chunk), dtype=np.int64)])
+        flags, count, total = msf_kruskal(E[ids], n)
+        carried = ids[flags]
+    in_msf = np.zeros(m, bool)
+    in_msf[carried] = True
+    return in_msf, count, total
+
+
 def msf_bytes(m_r, n_r, n: int, components: int) -> int:
     """Algorithmic bytes of one MSF solve:
     sum_r (32 m_r + 16 m_{r+1}) + 16 sum_r n_r + 12 (n - c)."""

@@ -121,6 +121,8 @@ SIGNATURES = {
     "phem_msf_solve": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, _VP, C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64), C.POINTER(MSFStats)]),
     "phem_msf_solve_device": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, _VP, _VP, C.POINTER(MSFStats)]),
+    "phem_msf_stream": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, C.c_uint64, _VP, C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_uint64), C.POINTER(C.c_float)]),
     "phem_msf_solve_csr": (C.c_int, [_VP, _VP, _VP, C.c_uint32, _VP, C.c_uint64, _VP, C.POINTER(C.c_uint64),
                                      C.POINTER(C.c_uint64), C.POINTER(MSFStats)]),
     "phem_csr_to_coo": (C.c_int, [_VP, _VP, _VP, C.c_int32, _VP, C.POINTER(C.c_int64)]),

@@ -279,6 +279,27 @@ class Context:
                                           C.byref(st)), "phem_msf_solve_device")
         return _msf_result(None, int(st.msf_edges), int(st.total_weight), st)
 
+    def msf_stream(self, edges, n: int, chunk: int, want_edges: bool = True, out=None) -> MSFResult:
+        """Chunked MSF (streamline_boruvka): the same forest as msf_solve,
+        solved chunk by chunk with the forest carried over, so the edge count
+        is not limited to 2^32.  `edges` is (m, 3) host (pinned for overlap) or
+        device records; device_ms is the time from the first copy to the last
+        solve; rounds and per-round counts are not reported."""
+        if isinstance(edges, np.ndarray):
+            edges = as_edges(edges)
+            m = len(edges)
+        else:
+            m = int(edges.shape[0])
+        if out is not None:
+            out = as_edges(out) if isinstance(out, np.ndarray) else out
+        elif want_edges:
+            out = np.empty((max(n - 1, 1), 3), np.uint32)
+        cnt, tot, ms = C.c_uint64(), C.c_uint64(), C.c_float()
+        check(lib().phem_msf_stream(self._h, ptr(edges), m, n, chunk, ptr(out), C.byref(cnt), C.byref(tot),
+                                    C.byref(ms)), "phem_msf_stream")
+        k = int(cnt.value)
+        return MSFResult(out[:k] if out is not None else None, k, int(tot.value), 0, device_ms=float(ms.value))
+
     def msf_solve_csr(self, offsets, cols, n: int, weights, m_upper: int) -> MSFResult:
         out = np.empty((max(n - 1, 1), 3), np.uint32)
         cnt, tot = C.c_uint64(), C.c_uint64()

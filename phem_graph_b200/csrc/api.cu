@@ -759,13 +759,13 @@ static phem_status msf_common(phem_context *ctx, const phem_edge *edges, uint64_
         set_error("msf: need 0 < n < 2^32 - 1, m <= 2^32 - 2^24 and an edge array");
         return PHEM_ERR_INVALID;
     }
+    const bool aligned_dev = is_device_ptr(edges) && (((uintptr_t)edges & 15) == 0);
     const size_t eb = (size_t)m * sizeof(phem_edge), ob = (size_t)n * sizeof(phem_edge);
-    const size_t o_edges = 0, o_out = align256(eb);
+    const size_t o_edges = 0, o_out = aligned_dev ? 0 : align256(eb);  // edges read in place: no staging area
     size_t base = 0;
     MsfPlan plan;
     PHEM_TRY(msf_plan(ctx, kKindMsf, nullptr, m, n, o_out + align256(ob), &plan, &base));
     Staged se, so;
-    const bool aligned_dev = is_device_ptr(edges) && (((uintptr_t)edges & 15) == 0);
     if (aligned_dev) {
         se.dev = const_cast<phem_edge *>(edges);
     } else {
@@ -832,6 +832,131 @@ phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, u
     }
     DeviceGuard g(ctx->device);
     return msf_common(ctx, d_edges, m, n, d_msf, nullptr, nullptr, stats, d_count_total);
+}
+
+// Chunked MSF (streamline_boruvka, MST/src/kernels.cu:849-1154): chunk k is
+// solved together with the forest of chunks 0..k-1, since under a strict total
+// order MSF(G1 + G2) = MSF(MSF(G1) + G2).  Each solve orders its input by
+// (w, position).  The carried forest sits directly before the chunk, ascending
+// by global edge index, and every one of its edges precedes every chunk edge
+// globally, so position order is global index order and the final forest is
+// exactly phem_msf_solve's.  Layout in the context's input buffer: two slots of
+// [R forest records | chunk records] and an output area of R records, with
+// R = n - 1 rounded up to 4 records so the chunk and every solve input start
+// 16-byte aligned; up to 3 zero records (self-loops, ignored) pad the gap
+// between the rounded start and the forest.  Chunk k + 1 is copied on the copy
+// stream while chunk k is solved.
+phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_t m, uint32_t n, uint64_t chunk,
+                            phem_edge *msf, uint64_t *count, uint64_t *total, float *ms)
+{
+    PHEM_TRY(check_ctx(ctx));
+    const uint64_t R = ((uint64_t)n + 2) & ~3ull;  // n - 1 rounded up to a multiple of 4
+    if (n == 0 || n == UINT32_MAX || chunk == 0 || (m > 0 && !h_edges) || R >= kMaxEdges ||
+        chunk > kMaxEdges - R) {
+        set_error("msf_stream: need 0 < n < 2^32 - 1, 0 < chunk <= 2^32 - 2^24 - (n - 1 rounded up to 4), edges");
+        return PHEM_ERR_INVALID;
+    }
+    if (count)
+        *count = 0;
+    if (total)
+        *total = 0;
+    if (ms)
+        *ms = 0.f;
+    if (m == 0)
+        return PHEM_OK;
+    DeviceGuard g(ctx->device);
+    const uint64_t top = std::min(chunk, m);  // largest chunk
+    const size_t slot_bytes = align256((R + top) * sizeof(phem_edge));
+    PHEM_TRY(input_reserve(ctx, 2 * slot_bytes + align256(R * sizeof(phem_edge)) + 256));
+    {
+        // size the solve workspace once for the largest solve (a later growth
+        // would free memory, which waits for the copies in flight)
+        MsfPlan plan;
+        PHEM_TRY(msf_plan(ctx, kKindMsf, nullptr, R + top, n, align256((size_t)n * sizeof(phem_edge)), &plan,
+                          nullptr));
+    }
+    char *b = static_cast<char *>(ctx->input);
+    phem_edge *slot[2] = {reinterpret_cast<phem_edge *>(b), reinterpret_cast<phem_edge *>(b + slot_bytes)};
+    phem_edge *d_out = reinterpret_cast<phem_edge *>(b + 2 * slot_bytes);
+    const uint64_t chunks = (m + chunk - 1) / chunk;
+    cudaEvent_t copied[2] = {nullptr, nullptr}, t0 = nullptr, t1 = nullptr;
+    phem_status st = PHEM_OK;
+    for (auto *e : {&copied[0], &copied[1], &t0, &t1})
+        if (cudaEventCreateWithFlags(e, (e == &t0 || e == &t1) ? cudaEventDefault : cudaEventDisableTiming) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            *e = nullptr;
+            st = PHEM_ERR_CUDA;
+        }
+    // the first copy waits for earlier work on the context stream, which may
+    // still read the input buffer
+    if (st == PHEM_OK && (cudaEventRecord(t0, ctx->stream) != cudaSuccess ||
+                          cudaStreamWaitEvent(ctx->copy_stream, t0, 0) != cudaSuccess))
+        st = PHEM_ERR_CUDA;
+    if (st != PHEM_OK)
+        set_error("msf_stream: cannot set up events: %s", cudaGetErrorString(cudaGetLastError()));
+    auto issue = [&](uint64_t k) -> phem_status {
+        const uint64_t off = k * chunk, len = std::min(chunk, m - off);
+        if (cudaMemcpyAsync(slot[k & 1] + R, h_edges + off, len * sizeof(phem_edge), cudaMemcpyDefault,
+                            ctx->copy_stream) != cudaSuccess ||
+            cudaEventRecord(copied[k & 1], ctx->copy_stream) != cudaSuccess) {
+            set_error("msf_stream: chunk copy failed: %s", cudaGetErrorString(cudaGetLastError()));
+            return PHEM_ERR_CUDA;
+        }
+        return PHEM_OK;
+    };
+    uint64_t carried = 0, weight = 0;  // forest of the chunks solved so far
+    if (st == PHEM_OK)
+        st = issue(0);
+    for (uint64_t k = 0; st == PHEM_OK && k < chunks; k++) {
+        // slot (k + 1) & 1 was last read by solve k - 1, which has returned
+        if (k + 1 < chunks && (st = issue(k + 1)) != PHEM_OK)
+            break;
+        phem_edge *cur = slot[k & 1];
+        const uint64_t len = std::min(chunk, m - k * chunk);
+        const uint64_t start = (R - carried) & ~3ull;
+        if (cudaStreamWaitEvent(ctx->stream, copied[k & 1], 0) != cudaSuccess ||
+            (R - carried > start && cudaMemsetAsync(cur + start, 0, (R - carried - start) * sizeof(phem_edge),
+                                                    ctx->stream) != cudaSuccess)) {
+            set_error("msf_stream: cannot queue chunk %llu", (unsigned long long)k);
+            st = PHEM_ERR_CUDA;
+            break;
+        }
+        st = msf_common(ctx, cur + start, R - start + len, n, d_out, &carried, &weight, nullptr, nullptr);
+        // the forest goes directly before the next chunk
+        if (st == PHEM_OK && k + 1 < chunks && carried &&
+            cudaMemcpyAsync(slot[(k + 1) & 1] + R - carried, d_out, carried * sizeof(phem_edge),
+                            cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess) {
+            set_error("msf_stream: cannot carry the forest");
+            st = PHEM_ERR_CUDA;
+        }
+    }
+    float t = 0.f;
+    if (st == PHEM_OK && (cudaEventRecord(t1, ctx->stream) != cudaSuccess ||
+                          (msf && carried &&
+                           cudaMemcpyAsync(msf, d_out, carried * sizeof(phem_edge), cudaMemcpyDefault,
+                                           ctx->stream) != cudaSuccess))) {
+        set_error("msf_stream: cannot copy the forest out");
+        st = PHEM_ERR_CUDA;
+    }
+    if (st == PHEM_OK)
+        st = stream_wait(ctx);
+    if (st == PHEM_OK && cudaEventElapsedTime(&t, t0, t1) != cudaSuccess)
+        t = 0.f;
+    if (st != PHEM_OK)
+        cudaStreamSynchronize(ctx->copy_stream);  // no copy may still land in the input buffer
+    for (auto e : {copied[0], copied[1], t0, t1})
+        if (e)
+            cudaEventDestroy(e);
+    if (st != PHEM_OK)
+        return st;
+    if (count)
+        *count = carried;
+    if (total)
+        *total = weight;
+    if (ms)
+        *ms = t;
+    return PHEM_OK;
 }
 
 phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, uint32_t n,

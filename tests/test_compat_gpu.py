@@ -56,3 +56,26 @@ def test_reference_mst_entry_points_on_libphem(tmp_path):
     assert (int(host.group(1)), int(host.group(2))) == (cnt, tot)
     assert (int(dev.group(1)), int(dev.group(2))) == (cnt, tot)
     assert int(dev.group(3)) == g.n - cnt
+
+
+@pytest.mark.skipif(not (REF / "mst_stream_phem").exists(), reason="compat drivers not built (reference tree absent)")
+@pytest.mark.parametrize("chunks", [1, 3, 7])
+def test_reference_streamline_mode_on_libphem(tmp_path, chunks):
+    """streamline_boruvka through the compat layer, fed by the reference's own
+    MatrixMarket chunk reader: the forest file holds the oracle's MSF (ascending
+    by edge id, 1-based endpoints) and the printed total weight is its total,
+    on both timed iterations."""
+    g = gen.rmat_graph(12, 8, seed=21, bits=6)
+    E = g.msf_edges()
+    flags, cnt, tot = oracle.msf_kruskal(E, g.n)
+    path, res = tmp_path / "g.mtx", tmp_path / "forest.txt"
+    io.write_mtx(path, E, g.n)
+    out = subprocess.run([str(REF / "mst_stream_phem"), str(path), str(chunks), str(res)], capture_output=True,
+                         text=True, timeout=300, cwd=tmp_path)  # the reader writes a temporary copy in its cwd
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    totals = [int(x) for x in re.findall(r"final weight by streamline approach (\d+)", out.stdout)]
+    assert totals == [tot, tot]
+    got = np.loadtxt(res, dtype=np.int64, ndmin=2)
+    want = E[flags].astype(np.int64)
+    want[:, :2] += 1
+    np.testing.assert_array_equal(got, want)

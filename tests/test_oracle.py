@@ -131,3 +131,27 @@ def test_msf_restatement_equals_serial_kruskal_tiny(seed):
     E = np.stack([rng.integers(0, n, m), rng.integers(0, n, m), rng.integers(1, 4, m)], 1).astype(np.uint32)
     flags, _, _ = oracle.msf_kruskal(E, n)
     np.testing.assert_array_equal(oracle.ref_serial_mst(E), np.nonzero(flags)[0])
+
+
+@pytest.mark.parametrize("scale,ef,bits,chunk", [(10, 16, 20, 1000), (11, 8, 2, 777), (9, 4, 1, 1), (12, 16, 20, 1 << 20)])
+def test_chunked_msf_restatement_equals_whole_graph(scale, ef, bits, chunk):
+    """streamline_boruvka's merge (MSF of each chunk plus the forest so far)
+    gives the whole graph's MSF: same edge set under (w, id), same weight --
+    heavy ties (1- and 2-bit weights), one-edge chunks and a single chunk."""
+    from phem_graph_b200 import gen
+    g = gen.rmat_graph(scale, ef, seed=scale + chunk, bits=bits)
+    E = g.msf_edges()
+    want, cnt, tot = oracle.msf_kruskal(E, g.n)
+    got, c2, t2 = oracle.msf_chunked(E, g.n, chunk)
+    np.testing.assert_array_equal(got, want)
+    assert (c2, t2) == (cnt, tot)
+
+
+@need_ref
+def test_chunked_msf_restatement_equals_pbbs_with_self_loops():
+    rng = np.random.default_rng(11)
+    n, m = 300, 5000
+    E = np.stack([rng.integers(0, n, m), rng.integers(0, n, m), rng.integers(1, 5, m)], 1).astype(np.uint32)
+    E[::50, 1] = E[::50, 0]  # self-loops
+    got, _, _ = oracle.msf_chunked(E, n, 613)
+    np.testing.assert_array_equal(np.sort(oracle.ref_pbbs_mst(E)), np.nonzero(got)[0])
