@@ -48,6 +48,9 @@ def test_null_context_is_invalid():
     st = lib.phem_cc_solve(None, None, 0, 1, None, None, 0, None)
     assert st == _lib.PHEM_ERR_INVALID
     assert b"context" in lib.phem_last_error()
+    for fn, args in (("phem_msf_solve", (None, None, 0, 1, None, None, None, None)),
+                     ("phem_msf_stream", (None, None, 0, 1, 16, None, None, None, None))):
+        assert getattr(lib, fn)(*args) == _lib.PHEM_ERR_INVALID, fn
 
 
 @pytest.mark.skipif(HAVE_GPU, reason="checks the no-device error path")
