@@ -29,6 +29,9 @@ On one GPU the same JSON line also carries the metric's other workloads:
   served   Poisson request streams at 1k-100k req/s through the serving loop
            (p50 / p99 latency, throughput), against serial one-graph solves.
 
+Host only: `python bench.py --ingest-only SCALE` times the MatrixMarket reader
+against the reference's own reader and exits.
+
 Multi-GPU (torchrun, one rank per GPU): every rank solves its own shard of a
 global multigraph (same vertex set, seed 22 + rank, 2^26 draws each), the local
 forests are all-gathered over NCCL and every rank solves their union; value =
@@ -576,6 +579,45 @@ def bench_msf_chunked_large(ctx, torch, scale: int, edge_factor: int = 16, chunk
                        "weights_sum_to_total": total_ok}}
 
 
+def bench_ingest(scale: int, reps: int = 3) -> dict:
+    """Host-side ingest: phem_read_mtx on the MatrixMarket file of an R-MAT
+    graph (edge factor 16, weights uniform in [1, 2^20], written to a
+    temporary directory first), median of `reps` reads, beside the MST
+    driver's own reader (getGraphInfo + mmapPopulateEdgeArray,
+    MST/src/utils.cu, compiled into oracle/_ref) on the same file and host
+    cores; the two outputs must be identical."""
+    import tempfile
+
+    import oracle
+    from phem_graph_b200 import gen, io
+    g = gen.rmat_graph(scale, 16, seed=3)
+    E = g.msf_edges()
+    with tempfile.TemporaryDirectory() as d:
+        path = Path(d) / "g.mtx"
+        io.write_mtx(path, E, g.n)
+        size = path.stat().st_size
+        ours, theirs, same = [], [], None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            a, _ = io.read_mtx(path)
+            ours.append(time.perf_counter() - t0)
+            if oracle.ref_available():
+                t0 = time.perf_counter()
+                b, _ = oracle.ref_mtx_read(path)
+                theirs.append(time.perf_counter() - t0)
+                same = bool(np.array_equal(a, b))
+    t = statistics.median(ours)
+    line = {"metric": "MatrixMarket read", "unit": "MB/s", "value": size / t / 1e6, "higher_is_better": True,
+            "config": {"workload": f"mtx_rmat{scale}_ef16", "bytes": size, "m": len(E), "n": g.n},
+            "seconds": t, "cores": os.cpu_count(), "api": "phem_read_mtx (C ABI)"}
+    if theirs:
+        tr = statistics.median(theirs)
+        line["cpu_baseline"] = {"value": size / tr / 1e6, "unit": "MB/s", "seconds": tr, "cores": os.cpu_count(),
+                                "kind": "reference", "sample": "the same file, median of %d reads" % reps,
+                                "identical_records": same}
+    return line
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's own CPU path (PBBS mst()) on the same
     workload, all host threads; one step = one full solve."""
@@ -638,8 +680,14 @@ def main() -> None:
                          "host memory (scale 28: 4.29 G edges, beyond one solve's 2^32 limit)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the connected-components, batched and served workloads")
+    ap.add_argument("--ingest-only", type=int, default=0, metavar="SCALE",
+                    help="host only: time the MatrixMarket reader on an R-MAT graph of this scale against the "
+                         "reference's own reader, then exit (no GPU needed)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.ingest_only:
+        print(json.dumps(bench_ingest(args.ingest_only)))
+        return
     if args.impl == "reference":
         run_reference(args)
         return
