@@ -278,9 +278,9 @@ phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, u
  * scales with chunk + n, not m.
  *   msf (host or device, room for n - 1 records, may be NULL), *count, *total
  *   as phem_msf_solve; *ms = device time from the first copy to the last solve.
- * Needs 0 < chunk and chunk + n <= 2^32 - 2^24 (roughly).  h_edges may be host
- * (pinned for the copies to overlap) or device memory.  count, total and ms
- * may be NULL. */
+ * Needs 0 < chunk <= 2^32 - 2^24 - R, with R = n - 1 rounded up to a multiple
+ * of 4 (else INVALID).  h_edges may be host (pinned for the copies to overlap)
+ * or device memory.  count, total and ms may be NULL. */
 phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_t m, uint32_t n, uint64_t chunk,
                             phem_edge *msf, uint64_t *count, uint64_t *total, float *ms);
 
