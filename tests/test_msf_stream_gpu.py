@@ -8,8 +8,10 @@ import pytest
 import oracle
 import phem_graph_b200 as P
 from phem_graph_b200 import _lib, gen
+from tests.golden import load, names
 
 pytestmark = pytest.mark.gpu
+MSF_CASES = names("msf_")
 
 
 def expect(E, n):
@@ -20,6 +22,17 @@ def expect(E, n):
 def assert_msf(r, E, ids, cnt, tot):
     assert r.count == cnt and r.total == tot
     np.testing.assert_array_equal(r.edges, np.asarray(E, np.uint32).reshape(-1, 3)[ids])
+
+
+@pytest.mark.parametrize("name", MSF_CASES)
+def test_golden_in_chunks(ctx, name):
+    """Every golden MSF vector (PBBS mst() / serial Kruskal outputs of the
+    reference's own code) in one-edge (small cases), small ragged and
+    three-way chunks."""
+    g = load(name)
+    E, n = np.asarray(g["edges"], np.uint32).reshape(-1, 3), int(g["n"])
+    for chunk in sorted({1 if len(E) <= 6000 else 61, 7, max(1, len(E) // 3 + 1)}):
+        assert_msf(ctx.msf_stream(E, n, chunk), E, g["msf_ids"], int(g["count"]), int(g["total"]))
 
 
 @pytest.mark.parametrize("chunk", [1 << 18, 100_003, 4096, 1 << 30])
