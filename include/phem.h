@@ -240,10 +240,11 @@ phem_status phem_cc_merge(phem_context *ctx, const uint64_t *d_forest_a, const u
  *                  (DEVICE, may be NULL);
  *   stream      cudaStream_t the work is queued on (NULL: the default stream).
  * Runs on the current device and returns when the work is complete.
- * n > PHEM_CC_NOALLOC_MAX_VERTICES returns PHEM_ERR_INVALID.  The first call on
- * a device looks the scratch address up (make it before any stream capture).
- * All calls on a device share the scratch: calls that overlap in time race and
- * corrupt each other's results. */
+ * n > PHEM_CC_NOALLOC_MAX_VERTICES returns PHEM_ERR_INVALID.  Every call looks
+ * the scratch address up in the current CUDA context (no allocation); the first
+ * call on a device also loads the library's module there, so make it before any
+ * stream capture.  All calls on a device share the scratch: calls that overlap
+ * in time race and corrupt each other's results. */
 phem_status phem_cc_solve_noalloc(const uint64_t *d_edges, int64_t m, int32_t n, int32_t *d_labels,
                                   uint64_t *d_forest, void *stream);
 
@@ -276,8 +277,10 @@ phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, u
  * (w, edge index), ascending by edge index -- but m has no 2^32 limit: each
  * solve holds one chunk plus at most n - 1 forest edges, so device memory
  * scales with chunk + n, not m.
- *   msf (host or device, room for n - 1 records, may be NULL), *count, *total
- *   as phem_msf_solve; *ms = device time from the first copy to the last solve.
+ *   msf (host memory, or device memory of the context's device, room for
+ *   n - 1 records, may be NULL; checked before any chunk is solved), *count,
+ *   *total as phem_msf_solve; *ms = device time from the first copy to the
+ *   last solve.
  * Needs 0 < chunk <= 2^32 - 2^24 - R, with R = n - 1 rounded up to a multiple
  * of 4 (else INVALID).  h_edges may be host (pinned for the copies to overlap)
  * or device memory.  count, total and ms may be NULL. */

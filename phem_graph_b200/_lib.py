@@ -1,7 +1,10 @@
 """ctypes binding of libphem.so (include/phem.h).
 
 The library is the product: if it is missing this module raises instead of
-falling back to anything else.
+falling back to anything else.  The seeded input generators (phem_gen_*,
+host-only code) are also built alone into libphem_gen.so, which gen_lib()
+loads, so that generating an input does not map the solver library (the
+reference arm of the benchmark generates its input without it).
 """
 from __future__ import annotations
 
@@ -12,6 +15,7 @@ import numpy as np
 
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libphem.so"
+GEN_LIB_PATH = PKG / "libphem_gen.so"
 
 PHEM_OK = 0
 PHEM_ERR_INVALID = 1
@@ -174,6 +178,33 @@ def lib() -> C.CDLL:
             f.argtypes = args
         _lib = L
     return _lib
+
+
+_GEN_NAMES = ("phem_gen_mix64", "phem_gen_er", "phem_gen_rmat", "phem_gen_weights", "phem_pack_msf_edges",
+              "phem_csr_from_sorted_pairs", "phem_gen_rmat_range", "phem_gen_rgg")
+_gen_lib = None
+
+
+def gen_lib() -> C.CDLL:
+    """The loaded libphem_gen.so (the generators alone); raises if it has not been built."""
+    global _gen_lib
+    if _gen_lib is None:
+        if not GEN_LIB_PATH.exists():
+            raise ImportError(f"{GEN_LIB_PATH} is missing: build it with `python -m phem_graph_b200.build`")
+        L = C.CDLL(str(GEN_LIB_PATH))
+        for name in _GEN_NAMES:
+            res, args = SIGNATURES[name]
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _gen_lib = L
+    return _gen_lib
+
+
+def check_gen(status: int, where: str) -> None:
+    """check() for the generator library (which keeps no error text)."""
+    if status != PHEM_OK:
+        raise PhemError(status, where, "invalid generator arguments")
 
 
 def check(status: int, where: str) -> None:

@@ -1,5 +1,5 @@
 """Builds libphem.so in-tree: the sm_100a CUDA kernels, the C ABI and the
-synthetic-input generators.
+synthetic-input generators; and libphem_gen.so, the generators alone.
 
     python -m phem_graph_b200.build            # incremental
     python -m phem_graph_b200.build --force    # rebuild everything
@@ -22,6 +22,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libphem.so"
+GEN_LIB = PKG / "libphem_gen.so"  # the host generators alone (no CUDA)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -87,6 +88,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         raise RuntimeError("libphem.so: compilation failed")
     if force or jobs or _stale(LIB, objs):
         _run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xcompiler", "-pthread"])
+    gen_obj = BUILD / "gen.cpp.o"
+    if force or _stale(GEN_LIB, [gen_obj]):
+        _run(["g++", "-shared", "-pthread", "-o", str(GEN_LIB), str(gen_obj)])
     return LIB
 
 

@@ -72,7 +72,7 @@ phem_context *context()
 // The heterogeneous CPU share is not part of this build: GPU_share must be 1.
 float SpanningTree(graph_data *h_input, graph_data *d_input, graph_data_host *)
 {
-    if ((int)GPU_share != 1) {
+    if (!(GPU_share == 1.0f)) {  // a float: 1.9 and 0.9999 are both a CPU share
         fprintf(stderr, "SpanningTree: GPU_share = %f; this build runs every edge on the GPU (use 1)\n",
                 (double)GPU_share);
         exit(EXIT_FAILURE);

@@ -100,6 +100,18 @@ bool is_device_ptr(const void *p)
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
+bool is_device_ptr_on(const void *p, int dev)
+{
+    if (!p)
+        return false;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) && attr.device == dev;
+}
+
 uint64_t next_epochs(phem_context *ctx, uint32_t count)
 {
     // Epochs are stored in 30 bits of a status word.  Before they wrap the
@@ -825,9 +837,9 @@ phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, u
                                   phem_edge *d_msf, uint64_t *d_count_total, phem_msf_stats *stats)
 {
     PHEM_TRY(check_ctx(ctx));
-    if (!is_device_ptr(d_edges) || (d_msf && !is_device_ptr(d_msf)) ||
-        (d_count_total && !is_device_ptr(d_count_total))) {
-        set_error("msf_solve_device: arrays must be device memory");
+    if (!is_device_ptr_on(d_edges, ctx->device) || (d_msf && !is_device_ptr_on(d_msf, ctx->device)) ||
+        (d_count_total && !is_device_ptr_on(d_count_total, ctx->device))) {
+        set_error("msf_solve_device: arrays must be device memory of the context's device %d", ctx->device);
         return PHEM_ERR_INVALID;
     }
     DeviceGuard g(ctx->device);
@@ -862,6 +874,12 @@ phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_
         *total = 0;
     if (ms)
         *ms = 0.f;
+    // a device output must be this context's device memory: checked before
+    // the stream is solved, not at the final copy
+    if (msf && is_device_ptr(msf) && !is_device_ptr_on(msf, ctx->device)) {
+        set_error("msf_stream: the output is device memory of another device than the context's %d", ctx->device);
+        return PHEM_ERR_INVALID;
+    }
     if (m == 0)
         return PHEM_OK;
     DeviceGuard g(ctx->device);

@@ -118,6 +118,8 @@ phem_status ctl_status(uint32_t err, const char *what);
 
 // True when p is device (or managed) memory of the current device.
 bool is_device_ptr(const void *p);
+// True when p is device (or managed) memory of device `dev`.
+bool is_device_ptr_on(const void *p, int dev);
 
 uint64_t next_epochs(phem_context *ctx, uint32_t count);
 

@@ -20,16 +20,17 @@
 //   * n <= PHEM_CC_NOALLOC_MAX_VERTICES (2^20).  The scratch is 4 MiB of
 //     parent words plus one status word, reserved when the CUDA module of this
 //     file is loaded; larger n is rejected with PHEM_ERR_INVALID.
-//   * The first call on a device does the set-up: with that device current it
-//     looks the scratch address up (cudaGetSymbolAddress, which also loads
-//     this file's module).  Make that first call before any stream capture.
+//   * Every call looks the scratch address up with the call's device current
+//     (cudaGetSymbolAddress: a table lookup, no allocation), so an address is
+//     never carried over from an earlier CUDA context of that device (after a
+//     cudaDeviceReset, or under a different driver context).  The first call
+//     on a device also loads this file's module: make that first call before
+//     any stream capture.
 //   * Every call on one device uses the same scratch.  Calls that overlap in
 //     time (two host threads, or two streams with work in flight at once)
 //     race on it and corrupt each other's results; serialise them.
 //   * The status word must start at zero; the init kernel clears it at the
 //     start of every call, before any other kernel of the call can set it.
-#include <mutex>
-
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -38,7 +39,6 @@ namespace phem {
 namespace {
 
 constexpr int32_t kNoallocMaxVertices = PHEM_CC_NOALLOC_MAX_VERTICES;
-constexpr int kNoallocMaxDevices = 64;
 
 static_assert(kNoallocMaxVertices == (1 << 20), "scratch size is part of the documented limit");
 
@@ -139,28 +139,17 @@ __global__ void __launch_bounds__(kBlock) na_label_kernel(int32_t n, int32_t *pa
 struct NoallocScratch {
     int32_t *parent = nullptr;
     uint32_t *status = nullptr;
-    int sm_count = 0;
 };
 
-std::mutex g_noalloc_mu;
-NoallocScratch g_noalloc_scratch[kNoallocMaxDevices];
-
-// Scratch addresses on device `dev` (the current device), looked up once.
-phem_status noalloc_scratch(int dev, NoallocScratch *out)
+// Scratch addresses in the CUDA context current on this thread (the call's
+// device), looked up on every call.
+phem_status noalloc_scratch(NoallocScratch *out)
 {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    NoallocScratch &s = g_noalloc_scratch[dev];
-    if (!s.parent) {
-        void *parent = nullptr, *status = nullptr;
-        PHEM_CUDA_TRY(cudaGetSymbolAddress(&parent, g_noalloc_parent));
-        PHEM_CUDA_TRY(cudaGetSymbolAddress(&status, g_noalloc_status));
-        int sms = 0;
-        PHEM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        s.status = static_cast<uint32_t *>(status);
-        s.sm_count = sms;
-        s.parent = static_cast<int32_t *>(parent);
-    }
-    *out = s;
+    void *parent = nullptr, *status = nullptr;
+    PHEM_CUDA_TRY(cudaGetSymbolAddress(&parent, g_noalloc_parent));
+    PHEM_CUDA_TRY(cudaGetSymbolAddress(&status, g_noalloc_status));
+    out->parent = static_cast<int32_t *>(parent);
+    out->status = static_cast<uint32_t *>(status);
     return PHEM_OK;
 }
 
@@ -199,13 +188,9 @@ extern "C" phem_status phem_cc_solve_noalloc(const uint64_t *d_edges, int64_t m,
         set_error("cc_solve_noalloc: need m >= 0, device edges when m > 0, and device labels");
         return PHEM_ERR_INVALID;
     }
-    int dev = 0;
+    int dev = 0, sm_count = 0;
     PHEM_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoallocMaxDevices) {
-        set_error("cc_solve_noalloc: device %d is beyond the %d devices this entry point tracks", dev,
-                  kNoallocMaxDevices);
-        return PHEM_ERR_UNSUPPORTED;
-    }
+    PHEM_CUDA_TRY(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
     if ((m > 0 && (!on_device(d_edges, dev) || ((uintptr_t)d_edges & 15))) || !on_device(d_labels, dev) ||
         (d_forest && !on_device(d_forest, dev))) {
         set_error("cc_solve_noalloc: edges (16-byte aligned), labels and forest must be memory of the "
@@ -213,18 +198,18 @@ extern "C" phem_status phem_cc_solve_noalloc(const uint64_t *d_edges, int64_t m,
         return PHEM_ERR_INVALID;
     }
     NoallocScratch s;
-    PHEM_TRY(noalloc_scratch(dev, &s));
+    PHEM_TRY(noalloc_scratch(&s));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned long long *forest = reinterpret_cast<unsigned long long *>(d_forest);
 
-    na_init_kernel<<<na_grid(s.sm_count, n), kBlock, 0, st>>>(n, s.parent, forest, s.status);
+    na_init_kernel<<<na_grid(sm_count, n), kBlock, 0, st>>>(n, s.parent, forest, s.status);
     PHEM_CUDA_TRY(cudaGetLastError());
     if (m > 0) {
-        na_unite_kernel<<<na_grid(s.sm_count, (m + 1) / 2), kBlock, 0, st>>>(
+        na_unite_kernel<<<na_grid(sm_count, (m + 1) / 2), kBlock, 0, st>>>(
             reinterpret_cast<const unsigned long long *>(d_edges), m, n, s.parent, forest, s.status);
         PHEM_CUDA_TRY(cudaGetLastError());
     }
-    na_label_kernel<<<na_grid(s.sm_count, n), kBlock, 0, st>>>(n, s.parent, d_labels, s.status);
+    na_label_kernel<<<na_grid(sm_count, n), kBlock, 0, st>>>(n, s.parent, d_labels, s.status);
     PHEM_CUDA_TRY(cudaGetLastError());
     uint32_t status = 0;
     PHEM_CUDA_TRY(cudaMemcpyAsync(&status, s.status, sizeof(status), cudaMemcpyDeviceToHost, st));

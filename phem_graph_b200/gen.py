@@ -1,4 +1,5 @@
-"""Seeded synthetic graphs (host side, libphem's phem_gen_* entry points).
+"""Seeded synthetic graphs (host side: the phem_gen_* entry points, loaded from
+libphem_gen.so, which holds the generators alone).
 
 The reference benchmarks on graph files that are not shipped; these stand in
 with seeded inputs of the same shapes.  Every value is a pure function of
@@ -11,7 +12,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import check_gen as check, gen_lib as lib
 
 # R-MAT quadrant probabilities of the benchmark configurations (a, b, c; d = 1 - a - b - c)
 RMAT_ABC = (0.57, 0.19, 0.19)

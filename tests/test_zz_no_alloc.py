@@ -8,6 +8,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle
 from phem_graph_b200 import _lib, gen
 from phem_graph_b200.api import forest_set
 
@@ -37,6 +38,7 @@ def _solve(torch, pairs, n, stream, with_forest=True):
 def _check_against_solve(ctx, pairs, n, labels, forest):
     ref = ctx.cc_solve(pairs, n)
     np.testing.assert_array_equal(labels, ref.labels)
+    np.testing.assert_array_equal(labels, oracle.cc_solve(pairs, n)[0])  # and the oracle's, directly
     if forest is not None:
         # which edge wins a hooking race is not fixed: compare forests by
         # validity -- n - c edges, all taken from the input with u < v, and
