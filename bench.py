@@ -423,32 +423,51 @@ def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), per_rate: int 
                        "large_workers": 2, "pool_graphs": len(pool), "pool_edges": pool_edges}}
 
 
-def bench_streamed(ctx, torch, scale: int, edge_factor: int = 32, batch: int = 1 << 28) -> dict:
+def bench_streamed(ctx, torch, scale: int, edge_factor: int = 32, batch: int = 1 << 28, cpu: bool = True) -> dict:
     """Streaming spanning forest (the reference's SpanningTree): R-MAT at
     `scale` with edge_factor * 2^scale draws (seed 28, self-loops dropped,
-    unsorted, ~69 GB of pairs at scale 28) generated into pinned host memory
-    before timing, then streamed to the GPU in batches of `batch` pairs
-    through triple-buffered copies overlapped with the union kernels
-    (phem_cc_stream); device memory: parent + labels + forest + 3 batch
-    buffers.  Checked by size-independent properties: labels are min-id and
-    idempotent, the forest has n - components edges, and a sample of edges
-    joins equal labels."""
-    from phem_graph_b200 import _lib
+    unsorted, ~69 GB of pairs at scale 28), generated on the GPU batch by batch
+    (phem_gen_rmat_range_device, the host generator's exact stream) and copied
+    into pinned host memory before timing, then streamed to the GPU in batches
+    of `batch` pairs through triple-buffered copies overlapped with the union
+    kernels (phem_cc_stream); device memory: parent + labels + forest + 3 batch
+    buffers.  Parity: the reference's own host_spanning_tree
+    (CC/host_spanning_tree.cu:89, oracle/_ref) consumes the same batches in
+    the same order on all host cores, its state carried from batch to batch as
+    in the reference; its root of every vertex (the smallest id of the
+    component, by its max -> min hook rule) must equal our label bit for bit.
+    Also checked: the forest has n - components edges."""
+    import oracle
+    from phem_graph_b200 import gen
     n = 1 << scale
     draws = edge_factor << scale
-    h = torch.empty(draws, dtype=torch.int64).pin_memory()
-    base = h.data_ptr()
-    filled, chunk = 0, 1 << 28
+    need = 8 * draws + (16 << scale)
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    avail = int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    workload = f"stream_rmat{scale}_ef{edge_factor}_batch2^{batch.bit_length() - 1}"
+    if avail is not None and avail < need + (8 << 30):
+        return {"workload": workload, "skipped": f"host memory: {avail / 1e9:.0f} GB available, "
+                                                 f"{(need + (8 << 30)) / 1e9:.0f} GB needed"}
+    dev = torch.device("cuda", ctx.device)
     t_gen = time.perf_counter()
-    for first in range(0, draws, chunk):
-        cnt = __import__("ctypes").c_uint64()
-        _lib.check(_lib.lib().phem_gen_rmat_range(scale, first, min(chunk, draws - first), 0.57, 0.19, 0.19, 28,
-                                                  base + 8 * filled, __import__("ctypes").byref(cnt)),
-                   "phem_gen_rmat_range")
-        filled += cnt.value
+    h = torch.empty(draws, dtype=torch.int64, pin_memory=True)
+    gen_chunk = 1 << 28
+    buf = torch.empty(gen_chunk, dtype=torch.int64, device=dev)
+    filled = 0
+    for first in range(0, draws, gen_chunk):
+        k = gen.rmat_range_device(ctx, scale, first, min(gen_chunk, draws - first), 28, buf)
+        h[filled:filled + k].copy_(buf[:k])
+        filled += k
+    del buf
+    torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
     m = filled
-    dev = torch.device("cuda", ctx.device)
     parent = torch.empty(n, dtype=torch.int32, device=dev)
     label = torch.empty(n, dtype=torch.int32, device=dev)
     forest = torch.empty(n, dtype=torch.int64, device=dev)
@@ -465,22 +484,42 @@ def bench_streamed(ctx, torch, scale: int, edge_factor: int = 32, batch: int = 1
     ctx.cc_label(n, parent, label)
     torch.cuda.synchronize()
     ar = torch.arange(n, dtype=torch.int32, device=dev)
-    lab = label.long()
-    ok_min = bool((label <= ar).all()) and bool((label[lab] == label).all())
     comps = int((label == ar).sum())
     filled_slots = int((forest != 0x7FFFFFFF).sum())
-    idx = torch.randint(0, m, (1 << 20,), generator=torch.Generator().manual_seed(0))
-    smp = h[idx].to(dev)
-    su, sv = (smp >> 32).long(), (smp & 0xFFFFFFFF).long()
-    ok_edges = bool((label[su] == label[sv]).all())
-    return {"workload": f"stream_rmat{scale}_ef{edge_factor}_batch2^{batch.bit_length() - 1}", "n": n, "m": m,
-            "unit": UNIT, "value": m / (ms / 1e3) / 1e9, "ms": ms, "generation_s": t_gen,
-            "roofline": {"bound": "host link", "achieved": 8 * m / (ms / 1e3) / 1e9, "peak": h2d_gbs,
-                         "unit": "GB/s", "frac": 8 * m / (ms / 1e3) / 1e9 / h2d_gbs,
-                         "peak_source": "one pinned host-to-device copy of a batch, measured here"},
-            "device_bytes": 16 * n + 3 * 8 * batch, "components": comps,
-            "checks": {"labels_min_id_idempotent": ok_min, "forest_edges_eq_n_minus_c": filled_slots == n - comps,
-                       "sampled_edges_join_equal_labels": ok_edges}}
+    del parent, forest, ar
+    out = {"workload": workload, "n": n, "m": m, "unit": UNIT, "value": m / (ms / 1e3) / 1e9, "ms": ms,
+           "generation_s": t_gen, "generator": "phem_gen_rmat_range_device (the host stream, on the GPU)",
+           "roofline": {"bound": "host link", "achieved": 8 * m / (ms / 1e3) / 1e9, "peak": h2d_gbs,
+                        "unit": "GB/s", "frac": 8 * m / (ms / 1e3) / 1e9 / h2d_gbs,
+                        "peak_source": "one pinned host-to-device copy of a batch, measured here"},
+           "device_bytes": 16 * n + 3 * 8 * batch, "components": comps,
+           "checks": {"forest_edges_eq_n_minus_c": filled_slots == n - comps}}
+    if cpu and oracle.ref_available():
+        ref = oracle.RefCC(n)
+        t_ref = 0.0
+        for off in range(0, m, batch):
+            ref.set_edges(hv[off:off + batch])
+            t_ref += ref.run()
+        rp, _ = ref.state()
+        workers = ref.workers()
+        ref.close()
+        # the reference's root of every vertex, by pointer jumping over its parents on the device
+        P = torch.from_numpy(rp).to(dev).long()
+        del rp
+        for _ in range(64):
+            Q = P[P]
+            if torch.equal(Q, P):
+                break
+            P = Q
+        del Q
+        out["checks"]["labels_equal_reference"] = bool(torch.equal(P.int(), label))
+        out["cpu_baseline"] = {"value": m / t_ref / 1e9, "unit": UNIT, "cores": workers, "kind": "reference",
+                               "sample": f"host_spanning_tree (CC/host_spanning_tree.cu) fed the same {m} pairs in "
+                                         f"the same batches of {batch}, state carried over; call time only"}
+        del P
+    del label, h
+    torch.cuda.empty_cache()
+    return out
 
 
 def bench_msf_chunked(ctx, h_pinned, n: int, one_shot_s: float, expect: tuple, chunk: int = 1 << 24) -> dict:
@@ -732,8 +771,9 @@ def main() -> None:
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--stream-scale", type=int, default=0,
-                    help="also stream an R-MAT graph of this scale (edge factor 32) from pinned host memory")
+    ap.add_argument("--stream-scale", type=int, default=28,
+                    help="also stream an R-MAT graph of this scale (edge factor 32) from pinned host memory and "
+                         "check its labels against the reference's host_spanning_tree (0: skip)")
     ap.add_argument("--msf-stream-scale", type=int, default=0,
                     help="also solve an R-MAT graph of this scale (edge factor 16) by chunked MSF from pinned "
                          "host memory (scale 28: 4.29 G edges, beyond one solve's 2^32 limit)")
@@ -905,8 +945,11 @@ def main() -> None:
         line["cc"] = bench_cc(ctx, torch, peaks, args.steps, args.warmup, not args.no_cpu_baseline)
         line["batched"] = bench_batched(ctx, torch)
         line["served"] = bench_served(torch)
-    if rank == 0 and world == 1 and args.stream_scale:
-        line["streamed"] = bench_streamed(ctx, torch, args.stream_scale)
+    if rank == 0 and world == 1 and args.stream_scale and not args.no_extra:
+        try:
+            line["streamed"] = bench_streamed(ctx, torch, args.stream_scale, cpu=not args.no_cpu_baseline)
+        except (RuntimeError, MemoryError) as e:  # e.g. pinned host memory refused: report, keep the line
+            line["streamed"] = {"workload": f"stream_rmat{args.stream_scale}_ef32", "error": str(e)[:300]}
     if rank == 0 and world == 1 and args.msf_stream_scale:
         del h_pinned, h_out
         line["msf_chunked_large"] = bench_msf_chunked_large(ctx, torch, args.msf_stream_scale)

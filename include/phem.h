@@ -115,10 +115,8 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.filter_min_ratio"  filter only when m >= ratio * light edges      [2.0]
  *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
  *   "msf.next_batch"        rounds queued per later check                 [4]
- *   "msf.edge_items"        records per thread in the edge pass, 4 or 8   [8]
- *   "msf.cache_components"  list rounds that follow a round in which at most
- *                           this many components chose an edge pre-reduce
- *                           their offers in per-CTA shared memory     [262144]
+ *   "msf.edge_ctas_per_sm"  CTAs of 8 independent warps per SM in the edge
+ *                           pass, 1 to 4                                  [4]
  *   "cc.canonical_light_per_vertex"  msf.light_per_vertex for the
  *                           PHEM_CC_CANONICAL forest (light = first by index) [2]
  *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
@@ -507,6 +505,15 @@ phem_status phem_gen_rmat(uint32_t scale, uint64_t draws, double a, double b, do
  * huge graph batch by batch).  out needs `count` entries (NULL to count). */
 phem_status phem_gen_rmat_range(uint32_t scale, uint64_t first, uint64_t count, double a, double b, double c,
                                 uint64_t seed, uint64_t *out, uint64_t *out_m);
+
+/* phem_gen_rmat_range on the GPU: the identical draws, in the identical order,
+ * written to d_out (device memory of the context's device, room for `count`
+ * entries); *out_m receives the number written.  Returns when done.  Input
+ * generation for graphs too large to generate on the host (no reference
+ * counterpart; the reference reads its graphs from files). */
+phem_status phem_gen_rmat_range_device(phem_context *ctx, uint32_t scale, uint64_t first, uint64_t count,
+                                       double a, double b, double c, uint64_t seed, uint64_t *d_out,
+                                       uint64_t *out_m);
 
 /* w[i] = 1 + (SplitMix64 value i & (2^bits - 1)), i.e. uniform in [1, 2^bits]. */
 phem_status phem_gen_weights(uint64_t m, uint64_t seed, uint32_t bits, uint32_t *w);

@@ -145,6 +145,8 @@ SIGNATURES = {
                                         C.POINTER(C.c_uint64)]),
     "phem_io_last_error": (C.c_char_p, []),
     "phem_gen_rgg": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, _VP, _VP, C.POINTER(C.c_uint64)]),
+    "phem_gen_rmat_range_device": (C.c_int, [_VP, C.c_uint32, C.c_uint64, C.c_uint64, C.c_double, C.c_double,
+                                             C.c_double, C.c_uint64, _VP, C.POINTER(C.c_uint64)]),
     "phem_batch_solve": (C.c_int, [_VP, _VP, C.c_uint32, _VP, C.c_uint64, C.c_uint32, _VP, _VP, _VP, _VP,
                                    C.POINTER(BatchStats)]),
     "phem_batch_plan_create": (C.c_int, [_VP, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(_VP)]),

@@ -31,7 +31,8 @@ NVCC_FLAGS = ARCH + [
 ]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-I", str(ROOT / "include")]
 
-CU_SOURCES = ["api.cu", "cc.cu", "msf.cu", "csr.cu", "noalloc.cu", "batch.cu", "batch_api.cu", "server.cu"]
+CU_SOURCES = ["api.cu", "cc.cu", "msf.cu", "csr.cu", "noalloc.cu", "batch.cu", "batch_api.cu", "server.cu",
+              "gen_dev.cu"]
 CXX_SOURCES = ["gen.cpp", "io.cpp"]
 HEADERS = ["common.cuh", "internal.h", "batch.h"]
 

@@ -428,12 +428,11 @@ phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double v
         ctx->tune_first_batch = (int)value;
     } else if (k == "msf.next_batch" && value >= 1 && value <= PHEM_MAX_ROUNDS) {
         ctx->tune_next_batch = (int)value;
-    } else if (k == "msf.edge_items" && (value == 4 || value == 8)) {
-        ctx->tune_edge_items = (int)value;
+    } else if (k == "msf.edge_ctas_per_sm" && value >= 1 && value <= 4 && value == (int)value) {
+        ctx->tune_edge_ctas = (int)value;
+        ctx->kernels_ready = 0;  // the grid size is recomputed at the next solve
     } else if (k == "cc.canonical_light_per_vertex" && value >= 0 && value < 1e6) {
         ctx->tune_canonical_light = value;
-    } else if (k == "msf.cache_components" && value >= 0.0 && value < 4294967296.0) {
-        ctx->tune_cache_components = value;
     } else if (k == "cc.sample_per_vertex" && value >= 0.0 && value < 1e6) {
         ctx->tune_cc_sample = value;
     } else if (k == "batch.block_size" && (value == 256 || value == 512 || value == 1024)) {
@@ -463,14 +462,12 @@ phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *
         *value = ctx->tune_filter_min_ratio;
     else if (k == "cc.canonical_light_per_vertex")
         *value = ctx->tune_canonical_light;
-    else if (k == "msf.cache_components")
-        *value = ctx->tune_cache_components;
     else if (k == "msf.first_batch")
         *value = ctx->tune_first_batch;
     else if (k == "msf.next_batch")
         *value = ctx->tune_next_batch;
-    else if (k == "msf.edge_items")
-        *value = ctx->tune_edge_items;
+    else if (k == "msf.edge_ctas_per_sm")
+        *value = ctx->tune_edge_ctas;
     else if (k == "cc.sample_per_vertex")
         *value = ctx->tune_cc_sample;
     else if (k == "batch.block_size")

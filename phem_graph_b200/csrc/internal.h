@@ -44,11 +44,9 @@ struct phem_context {
     uint32_t timeout_ms = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     int edge_pass_blocks = 0;          // persistent grid sizes, from the occupancy API
-    int edge_pass_blocks4 = 0;
     uint32_t kernels_ready = 0;        // bit k: launch attributes of edge kind k are set
     int gather_blocks = 0;
-    int tune_edge_items = 8;             // records per thread in the MSF edge pass (4 or 8)
-    double tune_cache_components = 262144; // MSF list rounds cache offers per CTA up to this many components
+    int tune_edge_ctas = 4;              // MSF edge pass: CTAs (of 8 independent warps) per SM, 1 to 4
     // tuning knobs (phem_context_set_tuning)
     double tune_light_per_vertex = 0.5;  // light edges per vertex in the MSF filter (0: no filter)
     double tune_canonical_light = 2.0;   // the same for the canonical CC forest (edges by index)

@@ -62,7 +62,6 @@ struct RoundArgs {
     uint64_t *status;
     unsigned long long *forest;
     Ctl *ctl;
-    uint64_t cache_max;  // list rounds after at most this many choosing components cache offers per CTA
 };
 
 // An input record takes part in the forest: self-loops never do; packed CC
@@ -82,83 +81,35 @@ __device__ __forceinline__ unsigned long long e0_key(uint32_t w, uint64_t id)
     return KIND == kKindMsf ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
 }
 
-// Offers key to best[t] for the live lanes of a warp with a fire-and-forget
-// 64-bit atomicMin.  `guard` is an earlier read of best[t]: it may be stale but
-// never below the true value, so it only skips updates that could not win.
-// When every live lane has the same target (a hub's run in row-major input)
-// the warp reduces the key first (high word, then low word among the lanes
-// holding the minimum high word) and one lane does the atomic.
-__device__ __forceinline__ void offer_row(unsigned long long *best, uint32_t t, unsigned long long key, bool live,
-                                          unsigned long long guard)
+// Offers `key` to best[ta] and best[tb] for the live lanes of a warp.  Lanes
+// with the same target are grouped (__match_any_sync) and their keys reduced
+// (high word, then low word among the lanes holding the minimum high word)
+// so each group does one atomic: a hub's records arrive in runs.  The group
+// leader reads best[t] first and skips the atomic when its key cannot win;
+// the read may be stale but is never below the true value.  Both targets'
+// guard reads are issued before either atomic.  Fire-and-forget 64-bit
+// atomicMin; every lane of the warp calls this, converged.
+__device__ __forceinline__ void offer_pair(unsigned long long *best, uint32_t ta, uint32_t tb,
+                                           unsigned long long key, bool on)
 {
-    const unsigned act = __ballot_sync(0xffffffffu, live);
-    if (!act)
+    const unsigned act = __ballot_sync(0xffffffffu, on);
+    if (!on)
         return;
-    const int leader = __ffs(act) - 1;
-    const uint32_t t0 = __shfl_sync(0xffffffffu, t, leader);
-    if (__all_sync(0xffffffffu, !live || t == t0)) {
-        const uint32_t hi = live ? (uint32_t)(key >> 32) : 0xffffffffu;
-        const uint32_t lo = live ? (uint32_t)key : 0xffffffffu;
-        const uint32_t mhi = __reduce_min_sync(0xffffffffu, hi);
-        const uint32_t mlo = __reduce_min_sync(0xffffffffu, hi == mhi ? lo : 0xffffffffu);
-        const unsigned long long km = ((unsigned long long)mhi << 32) | mlo;
-        if ((int)lane_id() == leader && km < guard)
-            atomicMin(best + t0, km);
-    } else if (live && key < guard) {
-        atomicMin(best + t, key);
-    }
-}
-
-// Per-CTA shared-memory pre-reduction of offers for rounds with few live
-// components: most survivors of such rounds offer to a handful of hub
-// components, and the same best[] words then serialise on one L2 slice.
-// A root owns a slot (t mod kOfferSlots) once it claims it; offers to owned
-// slots are shared-memory atomicMin, the rest go to best[] directly, and the
-// slots are flushed to best[] when the CTA's tiles are done.  The slots live
-// in the last row of the two stage buffers, which list rounds leave free
-// (their tiles are one row shorter): more shared memory would take L1 from
-// the heavy pass's relabel gathers, which depend on it.
-constexpr int kOfferSlots = 512;  // tags: 2 KB in stage 0; keys: 4 KB in stage 1
-constexpr uint32_t kNoTag = 0xffffffffu;
-
-// Slot of t, claiming it when free; -1 when another root holds it.
-__device__ __forceinline__ int offer_slot(uint32_t *tags, uint32_t t)
-{
-    const int slot = (int)(t & (kOfferSlots - 1));
-    uint32_t tag = *(volatile uint32_t *)(tags + slot);
-    if (tag == kNoTag)
-        tag = atomicCAS(tags + slot, kNoTag, t);
-    return (tag == kNoTag || tag == t) ? slot : -1;
-}
-
-// offer_row with the shared-memory slots: a non-null `kp` (the slot's key)
-// takes the offer there.
-__device__ __forceinline__ void offer_row_cached(unsigned long long *best, unsigned long long *kp, uint32_t t,
-                                                 unsigned long long key, bool live, unsigned long long guard)
-{
-    const unsigned act = __ballot_sync(0xffffffffu, live);
-    if (!act)
-        return;
-    const int leader = __ffs(act) - 1;
-    const uint32_t t0 = __shfl_sync(0xffffffffu, t, leader);
-    if (__all_sync(0xffffffffu, !live || t == t0)) {
-        const uint32_t hi = live ? (uint32_t)(key >> 32) : 0xffffffffu;
-        const uint32_t lo = live ? (uint32_t)key : 0xffffffffu;
-        const uint32_t mhi = __reduce_min_sync(0xffffffffu, hi);
-        const uint32_t mlo = __reduce_min_sync(0xffffffffu, hi == mhi ? lo : 0xffffffffu);
-        const unsigned long long km = ((unsigned long long)mhi << 32) | mlo;
-        if ((int)lane_id() == leader) {
-            if (kp)
-                atomicMin(kp, km);
-            else if (km < guard)
-                atomicMin(best + t0, km);
-        }
-    } else if (live) {
-        if (kp)
-            atomicMin(kp, key);
-        else if (key < guard)
-            atomicMin(best + t, key);
-    }
+    const uint32_t hi = (uint32_t)(key >> 32), lo = (uint32_t)key;
+    const unsigned pa = __match_any_sync(act, ta);
+    const unsigned pb = __match_any_sync(act, tb);
+    const uint32_t ahi = __reduce_min_sync(pa, hi), bhi = __reduce_min_sync(pb, hi);
+    const uint32_t alo = __reduce_min_sync(pa, hi == ahi ? lo : 0xffffffffu);
+    const uint32_t blo = __reduce_min_sync(pb, hi == bhi ? lo : 0xffffffffu);
+    const uint32_t lane = lane_id();
+    const bool la = (int)lane == __ffs(pa) - 1, lb = (int)lane == __ffs(pb) - 1;
+    const unsigned long long ka = ((unsigned long long)ahi << 32) | alo, kb = ((unsigned long long)bhi << 32) | blo;
+    const unsigned long long ga = la ? __ldcg(best + ta) : 0ull;
+    const unsigned long long gb = lb ? __ldcg(best + tb) : 0ull;
+    if (la && ka < ga)
+        atomicMin(best + ta, ka);
+    if (lb && kb < gb)
+        atomicMin(best + tb, kb);
 }
 
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
@@ -274,344 +225,285 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
 }
 
 // One Boruvka round's edge pass: relabel + filter + compaction + per-root
-// minimum.  Tile k of a CTA is tile blockIdx.x + k * gridDim.x; stage k % 2 of
-// shared memory receives it by bulk copy one iteration ahead.  Threads read
-// a tile striped (record j * kBlock + tid), conflict-free for 8, 12 and
-// 16-byte records.  Survivor ranks inside the tile come from warp ballots and
-// a scan of the (row, warp) counts that every warp does itself; warp 0
-// reserves the tile's output range from the CTA's chunk of the list.
-// Two stages: a tile's bulk copy is issued one tile ahead, which was enough
-// to find the next tile ready on 99 % of waits with three stages; the third
-// stage's 32 KB per CTA went back to L1 (heavy pass 555 -> 526 us).
-constexpr int kStages = 2;
-constexpr unsigned long long kChunk = 4096;  // output records reserved per atomicAdd
-constexpr uint64_t kMaxEdgeCtasPerSm = 4;      // edge-pass grid bound (sizes the list padding)
+// minimum, in one streaming pass over the round's input (the caller's records
+// in round 0 and the heavy pass, the previous round's survivor list
+// otherwise).
+//
+// Every warp works alone: no CTA barrier anywhere.  A warp owns the warp
+// tiles gw, gw + GW, gw + 2 GW, ... (gw its global index, GW the grid's warp
+// count; kEpStageBytes of input each: 128 records of 12 bytes, 192 packed
+// pairs or 96 survivor records) and streams them through a two-stage
+// pipeline of its own: lane 0 issues a 1-D bulk copy (cp.async.bulk, no
+// multicast) of tile k + 1 into one stage while the warp reads tile k from
+// the other, completion tracked by a per-stage mbarrier.  Lanes read records
+// lane-striped from shared memory (12- and 16-byte strides are conflict-free),
+// relabel endpoints to roots (read-only L1/L2 gathers of parent[]), drop
+// internal and out-of-pass records, and append survivors by ballot rank to a
+// 64-entry ring in the warp's shared memory.  Whenever 32 survivors are
+// pending the warp flushes them: one atomicAdd reserves exactly 32 list slots
+// (the list has no padding), one coalesced 512-byte store writes them, and
+// their keys are offered to both roots (offer_pair).  A warp's last partial
+// ring is flushed the same way with its exact count.
+constexpr int kEpThreads = 256;
+constexpr int kEpWarps = kEpThreads / 32;
+constexpr int kEpMaxCtasPerSm = 4;   // 32 warps per SM; registers capped at 64 per thread
+constexpr int kEpStages = 2;
+constexpr uint32_t kEpStageBytes = 1536;
+constexpr uint32_t kRing = 64;       // survivors staged per warp
 
-template <int ITEMS>
-__host__ __device__ constexpr size_t stage_bytes()
+struct __align__(16) EpWarp {
+    unsigned char stage[kEpStages][kEpStageBytes];
+    uint4 ring[kRing];
+    unsigned long long bar[kEpStages];
+};
+
+// Records per warp tile for a record size.
+template <uint32_t REC>
+__host__ __device__ constexpr uint32_t ep_tile_recs()
 {
-    return (size_t)kBlock * ITEMS * 16;  // sized for the widest (16-byte) record
+    return kEpStageBytes / REC;
 }
-template <int ITEMS>
-__host__ __device__ constexpr size_t pipe_smem()
+static_assert(kEpStageBytes % 12 == 0 && kEpStageBytes % 16 == 0 && (kEpStageBytes / 12) % 32 == 0 &&
+                  (kEpStageBytes / 8) % 32 == 0 && (kEpStageBytes / 16) % 32 == 0,
+              "warp tiles hold whole rows of every record size, in 16-byte multiples");
+
+// Appends the lanes' survivors (keep) to the ring in lane order.
+__device__ __forceinline__ void ring_append(EpWarp &w, uint32_t &filled, bool keep, uint4 rec, uint32_t lane)
 {
-    return kStages * stage_bytes<ITEMS>();
+    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+    if (keep)
+        w.ring[(filled + __popc(mask & ((1u << lane) - 1u))) & (kRing - 1)] = rec;
+    filled += __popc(mask);
 }
 
-// Resident CTAs per SM: two for 8 records per thread (registers), three for
-// 4 (registers capped to fit).
-template <int KIND, int ITEMS>
-__global__ void __launch_bounds__(kBlock, ITEMS == 4 ? 3 : 2) edge_pass_kernel(RoundArgs a)
+// Writes the `cnt` (<= 32) oldest ring entries to the list and offers them.
+template <int KIND>
+__device__ __forceinline__ void ring_flush(const RoundArgs &a, uint4 *out, unsigned long long *len, EpWarp &w,
+                                           uint32_t &flushed, uint32_t cnt, uint32_t lane)
 {
-    constexpr int kCnt = ITEMS * kWarps;  // row/warp counts per tile
-    extern __shared__ __align__(128) unsigned char stage_mem[];
-    __shared__ uint64_t s_bar[kStages];
-    __shared__ uint32_t s_cnt[kCnt];
-    __shared__ unsigned long long s_base, s_base2;
-    __shared__ uint32_t s_split;
+    __syncwarp();  // the lanes' ring writes are visible
+    const bool on = lane < cnt;
+    const uint4 rec = on ? w.ring[(flushed + lane) & (kRing - 1)] : make_uint4(0, 0, 0, 0);
+    flushed += cnt;
+    unsigned long long base = 0;
+    if (lane == 0)
+        base = atomicAdd(len, (unsigned long long)cnt);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (on)
+        out[base + lane] = rec;
+    const unsigned long long key =
+        KIND == kKindMsf ? (((unsigned long long)rec.z << 32) | rec.w) : (unsigned long long)rec.w;
+    offer_pair(a.best, rec.x, rec.y, key, on);
+    __syncwarp();  // the ring slots just read may be written again
+}
+
+// Bounded wait of the whole warp for a stage's bulk copy.
+__device__ __forceinline__ bool ep_wait(unsigned long long *bar, uint32_t parity, uint32_t *err)
+{
+    bool ok = mbar_wait(reinterpret_cast<uint64_t *>(bar), parity, err);
+    return __all_sync(0xffffffffu, ok);
+}
+
+// Input tile (the caller's records): rows of 32 records, lane-striped.
+// LIGHT keeps key < threshold with the endpoints as roots (round 0: every
+// vertex is its own root); otherwise keeps key >= threshold between different
+// components after relabelling both endpoints (the heavy pass: parent[] is
+// fully compressed, so one hop reaches the root).
+template <int KIND, bool LIGHT>
+__device__ __forceinline__ void ep_input_tile(const RoundArgs &a, const unsigned char *stage, bool bulk,
+                                              uint64_t tbase, uint32_t rem, uint32_t thr_hi, uint32_t thr_lo,
+                                              EpWarp &w, uint32_t &filled, uint32_t &flushed, uint4 *out,
+                                              unsigned long long *len, uint32_t lane, bool &any_bad)
+{
+    constexpr uint32_t REC = KIND == kKindMsf ? 12u : 8u;
+    constexpr int ROWS = (int)(ep_tile_recs<REC>() / 32);
+    uint32_t u[ROWS], v[ROWS], wt[ROWS];
+    bool keep[ROWS];
+    const uint32_t id0 = (uint32_t)tbase;
+#pragma unroll
+    for (int j = 0; j < ROWS; j++) {
+        const uint32_t idx = j * 32 + lane;
+        const bool inb = idx < rem;
+        uint32_t x = 0, y = 0, z = 0;
+        if (KIND == kKindMsf) {
+            if (bulk) {
+                const uint32_t *p = reinterpret_cast<const uint32_t *>(stage) + 3 * idx;
+                x = p[0];
+                y = p[1];
+                z = p[2];
+            } else if (inb) {
+                const uint32_t *p = static_cast<const uint32_t *>(a.e0) + 3 * (tbase + idx);
+                x = __ldcs(p);
+                y = __ldcs(p + 1);
+                z = __ldcs(p + 2);
+            }
+        } else {
+            unsigned long long e = 0;
+            if (bulk)
+                e = reinterpret_cast<const unsigned long long *>(stage)[idx];
+            else if (inb)
+                e = __ldcs(static_cast<const unsigned long long *>(a.e0) + tbase + idx);
+            x = (uint32_t)(e >> 32);
+            y = (uint32_t)e;
+        }
+        const uint32_t id = id0 + idx;
+        const bool live = inb && e0_live<KIND>(x, y);
+        const bool bad = live && max(x, y) >= a.n;
+        any_bad |= bad;
+        // e0_key(w, id) < threshold, compared as (high word, low word)
+        const bool light = KIND == kKindMsf ? (z < thr_hi || (z == thr_hi && id < thr_lo))
+                                            : (thr_hi != 0 || id < thr_lo);
+        keep[j] = live && !bad && (LIGHT ? light : !light);
+        u[j] = x;
+        v[j] = y;
+        wt[j] = z;
+    }
+    if (!LIGHT) {
+        // all rows' gathers in flight together
+#pragma unroll
+        for (int j = 0; j < ROWS; j++)
+            if (keep[j]) {
+                u[j] = __ldg(a.parent + u[j]);
+                v[j] = __ldg(a.parent + v[j]);
+            }
+#pragma unroll
+        for (int j = 0; j < ROWS; j++)
+            keep[j] = keep[j] && u[j] != v[j];
+    }
+#pragma unroll
+    for (int j = 0; j < ROWS; j++) {
+        ring_append(w, filled, keep[j], make_uint4(u[j], v[j], wt[j], id0 + j * 32 + lane), lane);
+        if (filled - flushed >= 32)
+            ring_flush<KIND>(a, out, len, w, flushed, 32, lane);
+    }
+}
+
+// List tile (the previous round's survivors {root_u, root_v, w, id}): both
+// roots are relabelled by one hop (the compress pointed every root that
+// hooked at its new root) and records inside one component are dropped.
+template <int KIND>
+__device__ __forceinline__ void ep_list_tile(const RoundArgs &a, const uint4 *in, const unsigned char *stage,
+                                             bool bulk, uint64_t tbase, uint32_t rem, EpWarp &w, uint32_t &filled,
+                                             uint32_t &flushed, uint4 *out, unsigned long long *len, uint32_t lane)
+{
+    constexpr int ROWS = (int)(ep_tile_recs<16>() / 32);
+    uint4 rec[ROWS];
+    bool keep[ROWS];
+#pragma unroll
+    for (int j = 0; j < ROWS; j++) {
+        const uint32_t idx = j * 32 + lane;
+        keep[j] = idx < rem;
+        rec[j] = make_uint4(0, 0, 0, 0);
+        if (bulk)
+            rec[j] = reinterpret_cast<const uint4 *>(stage)[idx];
+        else if (keep[j])
+            rec[j] = __ldcs(in + tbase + idx);
+    }
+#pragma unroll
+    for (int j = 0; j < ROWS; j++)
+        if (keep[j]) {
+            rec[j].x = __ldg(a.parent + rec[j].x);
+            rec[j].y = __ldg(a.parent + rec[j].y);
+        }
+#pragma unroll
+    for (int j = 0; j < ROWS; j++) {
+        ring_append(w, filled, keep[j] && rec[j].x != rec[j].y, rec[j], lane);
+        if (filled - flushed >= 32)
+            ring_flush<KIND>(a, out, len, w, flushed, 32, lane);
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(RoundArgs a)
+{
+    __shared__ EpWarp s_warp[kEpWarps];
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const uint32_t src = *(volatile uint32_t *)&ctl->src;
-    // list rounds read tiles one row short, which frees the last row of every
-    // stage for the offer slots
-    const int rows = src == kSrcList ? ITEMS - 1 : ITEMS;
-    const uint32_t tile_recs = (uint32_t)rows * kBlock;
-    constexpr size_t kFreeRow = (size_t)(ITEMS - 1) * kBlock * 16;
-    uint32_t *s_tag = reinterpret_cast<uint32_t *>(stage_mem + kFreeRow);
-    unsigned long long *s_key0 = reinterpret_cast<unsigned long long *>(stage_mem + stage_bytes<ITEMS>() + kFreeRow);
-    auto slot_key = [&](int i) { return s_key0 + i; };
-    // list rounds with few components (those that chose an edge last round)
-    const bool cached = src == kSrcList && r > 0 && ctl->n_r[r - 1] <= a.cache_max;
-    if (cached)
-        for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
-            s_tag[i] = kNoTag;
-            *slot_key(i) = kKeyNone;
-        }
-    const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
-    const uint32_t thr_hi = (uint32_t)(thr >> 32), thr_lo = (uint32_t)thr;
-    const bool light_round = src == kSrcLight;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    EpWarp &w = s_warp[warp];
     const bool from_e0 = src != kSrcList;
-    const uint64_t stream_policy = l2_evict_first();  // inputs and lists are read once per pass
+    const uint32_t rec_bytes = from_e0 ? (KIND == kKindMsf ? 12u : 8u) : 16u;
+    const uint32_t tile_recs = kEpStageBytes / rec_bytes;
     const uint64_t count = from_e0 ? a.m : ctl->wl_len[r - 1];
     const uint4 *in = (r & 1) ? a.wl0 : a.wl1;  // WL[(r - 1) & 1]
     uint4 *out = (r & 1) ? a.wl1 : a.wl0;       // WL[r & 1]
-    const uint32_t rec_bytes = from_e0 ? (KIND == kKindMsf ? 12u : 8u) : 16u;
-    const uint32_t tile_bytes = tile_recs * rec_bytes;
+    unsigned long long *len = &ctl->wl_len[r];
     const char *src_base = from_e0 ? static_cast<const char *>(a.e0) : reinterpret_cast<const char *>(in);
     const uint64_t ntiles = (count + tile_recs - 1) / tile_recs;
     const uint64_t full_tiles = count / tile_recs;  // the partial last tile is read directly
-    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    // Output space is reserved in chunks of up to kChunk records per CTA (one
-    // atomicAdd per chunk, not per tile); a tile that does not fit finishes the
-    // current chunk and continues in the next.  The unused tail of the CTA's
-    // last chunk is filled with dead records {0, 0, 0, 0}, which the next pass
-    // drops (equal roots), so a list holds at most one chunk of padding per CTA.
-    // Owned by lane 31 of warp 0: chunk cursor, room left, survivors written.
-    unsigned long long chunk_next = 0, chunk_left = 0, live = 0;
+    const uint64_t gw = (uint64_t)blockIdx.x * kEpWarps + warp, GW = (uint64_t)gridDim.x * kEpWarps;
+    const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
+    const uint32_t thr_hi = (uint32_t)(thr >> 32), thr_lo = (uint32_t)thr;
+    const uint64_t policy = l2_evict_first();  // inputs and lists are read once per pass
 
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++)
-            mbar_init(&s_bar[s], 1);
+    if (lane == 0) {
+        for (int s = 0; s < kEpStages; s++)
+            mbar_init(reinterpret_cast<uint64_t *>(&w.bar[s]), 1);
         fence_mbar_init();
-        for (int s = 0; s < kStages - 1; s++) {
-            const uint64_t t = blockIdx.x + (uint64_t)s * gridDim.x;
-            if (t < full_tiles) {
-                mbar_arrive_expect_tx(&s_bar[s], tile_bytes);
-                bulk_copy_g2s_hint(stage_mem + s * stage_bytes<ITEMS>(), src_base + t * tile_bytes, tile_bytes,
-                                   &s_bar[s], stream_policy);
-            }
-        }
     }
-    __syncthreads();
-    uint32_t parity = 0;  // bit s: phase of stage s's barrier to wait for
+    __syncwarp();
+    auto issue = [&](uint64_t t, int s) {  // lane 0 only
+        mbar_arrive_expect_tx(reinterpret_cast<uint64_t *>(&w.bar[s]), kEpStageBytes);
+        bulk_copy_g2s_hint(w.stage[s], src_base + t * kEpStageBytes, kEpStageBytes,
+                           reinterpret_cast<uint64_t *>(&w.bar[s]), policy);
+    };
+    if (lane == 0 && gw < full_tiles)
+        issue(gw, 0);
+    uint32_t filled = 0, flushed = 0;  // ring cursors (warp-uniform)
+    uint32_t parity = 0;               // bit s: phase of stage s's barrier to wait for
+    uint32_t pending = gw < full_tiles ? 1u : 0u;  // bit s: a copy into stage s is in flight
+    bool any_bad = false, failed = false;
     int s = 0;
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, s = (s + 1 == kStages) ? 0 : s + 1) {
+    for (uint64_t t = gw; t < ntiles; t += GW, s ^= 1) {
+        // tile t + GW goes into the other stage, which the previous tile left
+        // (its reads were fenced against the async proxy before the warp
+        // synchronised at the end of that tile)
+        const uint64_t t2 = t + GW;
+        if (t2 < full_tiles) {
+            if (lane == 0)
+                issue(t2, s ^ 1);
+            pending |= 1u << (s ^ 1);
+        }
         const bool bulk = t < full_tiles;
-        bool ok = true;
         if (bulk) {
-            ok = mbar_wait(&s_bar[s], (parity >> s) & 1u, &ctl->err);
+            if (!ep_wait(&w.bar[s], (parity >> s) & 1u, &ctl->err)) {
+                failed = true;
+                break;
+            }
             parity ^= 1u << s;
+            pending &= ~(1u << s);
         }
-        if (__syncthreads_or(!ok))
-            break;  // a bulk copy never completed; the status bit is set
-        unsigned char *stage = stage_mem + s * stage_bytes<ITEMS>();
         const uint64_t tbase = t * tile_recs;
-        // per-record work in 32-bit arithmetic: edge ids are below 2^32
-        const uint64_t left64 = count - tbase;
-        const uint32_t rem = left64 < tile_recs ? (uint32_t)left64 : tile_recs;  // also excludes the free row
-        const uint32_t id0 = (uint32_t)tbase;
-        uint32_t ra[ITEMS], rb[ITEMS], w[ITEMS], id[ITEMS];
-        bool keep[ITEMS];
-        // Whole tiles are read from the stage with shared-memory loads (the
-        // branch is uniform over the tile); only the ragged last tile reads
-        // global memory.  Selecting one pointer from either space would make
-        // every record load a generic load.
-        if (from_e0) {
-            bool any_bad = false;
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++) {
-                const uint32_t idx = j * kBlock + threadIdx.x;
-                const bool inb = idx < rem;
-                id[j] = id0 + idx;
-                uint32_t u = 0, v = 0, ww = 0;
-                if (KIND == kKindMsf) {
-                    if (bulk) {
-                        const uint32_t *p = reinterpret_cast<const uint32_t *>(stage) + 3 * idx;
-                        u = p[0];
-                        v = p[1];
-                        ww = p[2];
-                    } else if (inb) {
-                        const uint32_t *p = static_cast<const uint32_t *>(a.e0) + 3 * (tbase + idx);
-                        u = p[0];
-                        v = p[1];
-                        ww = p[2];
-                    }
-                } else {
-                    unsigned long long e = 0;
-                    if (bulk)
-                        e = reinterpret_cast<const unsigned long long *>(stage)[idx];
-                    else if (inb)
-                        e = static_cast<const unsigned long long *>(a.e0)[tbase + idx];
-                    u = (uint32_t)(e >> 32);
-                    v = (uint32_t)e;
-                }
-                const bool live_e = inb && e0_live<KIND>(u, v);
-                const bool bad = live_e && max(u, v) >= a.n;
-                any_bad |= bad;
-                // e0_key(w, id) < thr, compared as (high word, low word)
-                const bool light = KIND == kKindMsf ? (ww < thr_hi || (ww == thr_hi && id[j] < thr_lo))
-                                                    : (thr_hi != 0 || id[j] < thr_lo);
-                keep[j] = live_e && !bad && (light_round ? light : !light);
-                ra[j] = u;
-                rb[j] = v;
-                w[j] = ww;
-            }
-            if (any_bad && light_round)
-                set_err(&ctl->err, kErrRange);
-        } else {
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++) {
-                const uint32_t idx = j * kBlock + threadIdx.x;
-                const bool inb = idx < rem;
-                uint4 rec = make_uint4(0, 0, 0, 0);
-                if (bulk) {
-                    if (inb)
-                        rec = reinterpret_cast<const uint4 *>(stage)[idx];
-                } else if (inb) {
-                    rec = __ldcs(in + (tbase + idx));
-                }
-                keep[j] = inb;
-                ra[j] = rec.x;
-                rb[j] = rec.y;
-                w[j] = rec.z;
-                id[j] = rec.w;
-            }
-        }
-        if (src != kSrcLight) {  // light round 0: every vertex is its own root
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++)
-                if (keep[j]) {
-                    ra[j] = __ldg(a.parent + ra[j]);
-                    rb[j] = __ldg(a.parent + rb[j]);
-                }
-        }
-        unsigned mask[ITEMS];
-#pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            keep[j] = keep[j] && ra[j] != rb[j];
-            mask[j] = __ballot_sync(0xffffffffu, keep[j]);
-        }
-        if (lane == 0)
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++)
-                s_cnt[j * kWarps + warp] = __popc(mask[j]);
-        __syncthreads();  // s_cnt complete; every record of the stage is in registers
-        if (threadIdx.x == 0) {
-            // refill the stage read last iteration with the next tile of this CTA
-            const uint64_t t2 = t + (uint64_t)(kStages - 1) * gridDim.x;
-            const int s2 = (s + kStages - 1) % kStages;
-            if (t2 < full_tiles) {
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&s_bar[s2], tile_bytes);
-                bulk_copy_g2s_hint(stage_mem + s2 * stage_bytes<ITEMS>(), src_base + t2 * tile_bytes, tile_bytes,
-                                   &s_bar[s2], stream_policy);
-            }
-        }
-        // Every warp scans the row/warp counts (row-major, kCnt / 32 per lane)
-        // itself, so the ranks need no barrier of their own; warp 0 also
-        // reserves the tile's output range, which the staging barrier below
-        // publishes before the dense phase reads it.
-        constexpr int kPer = kCnt / 32;
-        static_assert(kPer == 1 || kPer == 2, "row/warp counts per lane");
-        uint32_t c[kPer], sum = 0;
-#pragma unroll
-        for (int q = 0; q < kPer; q++) {
-            c[q] = s_cnt[kPer * lane + q];
-            sum += c[q];
-        }
-        uint32_t incl = sum;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= (uint32_t)d)
-                incl += y;
-        }
-        const uint32_t ex0 = incl - sum, ex1 = ex0 + c[0];
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        if (warp == 0 && lane == 31) {
-            s_base = chunk_next;
-            if (total <= chunk_left) {
-                s_split = total;
-                chunk_next += total;
-                chunk_left -= total;
-            } else {
-                // the first chunk_left survivors finish the current chunk, the
-                // rest open a new one sized to this CTA's remaining input
-                s_split = (uint32_t)chunk_left;
-                const unsigned long long rest = total - chunk_left;
-                const uint64_t tiles_left = (ntiles - 1 - t) / gridDim.x + 1;
-                const unsigned long long cap = tiles_left * tile_recs;
-                const unsigned long long want = cap < kChunk ? cap : kChunk;
-                const unsigned long long size = want > rest ? want : rest;
-                const unsigned long long fresh = atomicAdd(&ctl->wl_len[r], size);
-                s_base2 = fresh;
-                chunk_next = fresh + rest;
-                chunk_left = size - rest;
-            }
-            live += total;
-        }
-        // Stage the survivors densely, in rank (= input) order, in this
-        // tile's own stage buffer: its input is already in registers, and the
-        // buffer is refilled only after the next tile's second barrier.
-        uint4 *staging = reinterpret_cast<uint4 *>(stage);
-        const unsigned below = (1u << lane) - 1u;
-#pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            // exclusive offset of entry (row j, this warp): lane e / kPer holds it
-            const uint32_t e = j * kWarps + warp;
-            const uint32_t mine = (kPer == 2 && (e & 1)) ? ex1 : ex0;
-            const uint32_t off = __shfl_sync(0xffffffffu, mine, e / kPer);
-            if (mask[j] && keep[j])  // mask: warp-uniform skip of rows without survivors
-                staging[off + __popc(mask[j] & below)] = make_uint4(ra[j], rb[j], w[j], id[j]);
-        }
-        __syncthreads();  // staging, bases and split are ready
-        // Dense phase: coalesced survivor writes and the offers of both
-        // endpoints, several records per thread so the guard loads overlap.
-        const uint32_t split = s_split;
-        const unsigned long long base = s_base, base2 = s_base2;
-        for (uint32_t i0 = 0; i0 < total; i0 += kBlock * 4) {
-            uint4 rec[4];
-            bool on[4];
-            unsigned long long key[4], ga[4], gb[4];
-            unsigned long long *ka[4], *kb[4];
-            bool row[4];  // warp-uniform: this warp's row of the dense list holds a survivor
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                row[q] = i0 + q * kBlock + warp * 32 < total;
-                const uint32_t i = i0 + q * kBlock + threadIdx.x;
-                on[q] = row[q] && i < total;
-                ka[q] = kb[q] = nullptr;
-                ga[q] = gb[q] = 0ull;
-                rec[q] = make_uint4(0, 0, 0, 0);
-                key[q] = 0ull;
-                if (!row[q])
-                    continue;  // sparse input passes leave most rows empty
-                rec[q] = on[q] ? staging[i] : make_uint4(0, 0, 0, 0);
-                key[q] = ((unsigned long long)rec[q].z << 32) | rec[q].w;
-                const int sa = cached && on[q] ? offer_slot(s_tag, rec[q].x) : -1;
-                const int sb = cached && on[q] ? offer_slot(s_tag, rec[q].y) : -1;
-                ka[q] = sa >= 0 ? slot_key(sa) : nullptr;
-                kb[q] = sb >= 0 ? slot_key(sb) : nullptr;
-                ga[q] = on[q] && !ka[q] ? __ldcg(a.best + rec[q].x) : 0ull;
-                gb[q] = on[q] && !kb[q] ? __ldcg(a.best + rec[q].y) : 0ull;
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (!row[q])
-                    continue;
-                const uint32_t i = i0 + q * kBlock + threadIdx.x;
-                if (on[q])
-                    out[i < split ? base + i : base2 + (i - split)] = rec[q];
-                if (cached) {
-                    offer_row_cached(a.best, ka[q], rec[q].x, key[q], on[q], ga[q]);
-                    offer_row_cached(a.best, kb[q], rec[q].y, key[q], on[q], gb[q]);
-                } else {
-                    offer_row(a.best, rec[q].x, key[q], on[q], ga[q]);
-                    offer_row(a.best, rec[q].y, key[q], on[q], gb[q]);
-                }
-            }
-        }
-        // This thread's staging writes and reads of the stage come before the
-        // bulk copy that will refill it.  No barrier here: the next tile's
-        // opening barrier already orders this tile's reads of staging, s_cnt
-        // and the bases before anything rewrites them (the refill of this
-        // stage is issued after the next tile's second barrier).
-        fence_proxy_async_smem();
+        const uint64_t left = count - tbase;
+        const uint32_t rem = left < tile_recs ? (uint32_t)left : tile_recs;
+        if (src == kSrcList)
+            ep_list_tile<KIND>(a, in, w.stage[s], bulk, tbase, rem, w, filled, flushed, out, len, lane);
+        else if (src == kSrcLight)
+            ep_input_tile<KIND, true>(a, w.stage[s], bulk, tbase, rem, thr_hi, thr_lo, w, filled, flushed, out,
+                                      len, lane, any_bad);
+        else
+            ep_input_tile<KIND, false>(a, w.stage[s], bulk, tbase, rem, thr_hi, thr_lo, w, filled, flushed, out,
+                                       len, lane, any_bad);
+        fence_proxy_async_smem();  // this lane's reads of the stage precede its refill
+        __syncwarp();
     }
-    __syncthreads();  // the last tile's readers are done with the bases
-    if (cached) {  // flush the shared-memory slots to best[]
-        for (int i = threadIdx.x; i < kOfferSlots; i += kBlock) {
-            const uint32_t tag = s_tag[i];
-            if (tag != kNoTag) {
-                const unsigned long long k = *slot_key(i);
-                if (k < __ldcg(a.best + tag))
-                    atomicMin(a.best + tag, k);
-            }
-        }
+    if (failed) {
+        // a copy never completed (the status bit is set): wait, bounded, for
+        // every copy still in flight into this warp's stages before leaving
+        for (int q = 0; q < kEpStages; q++)
+            if (pending & (1u << q))
+                ep_wait(&w.bar[q], (parity >> q) & 1u, &ctl->err);
+        return;
     }
-    // pad the last chunk's unused tail with dead records and publish this
-    // CTA's exact survivor count
-    if (threadIdx.x == 31) {
-        s_base = chunk_next;
-        s_split = (uint32_t)chunk_left;
-        if (live)
-            atomicAdd(&ctl->m_r[r], live);
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < s_split; i += kBlock)
-        out[s_base + i] = make_uint4(0, 0, 0, 0);
+    if (filled != flushed)
+        ring_flush<KIND>(a, out, len, w, flushed, filled - flushed, lane);
+    if (__any_sync(0xffffffffu, any_bad) && lane == 0 && src == kSrcLight)
+        set_err(&ctl->err, kErrRange);
+    if (lane == 0 && filled)
+        atomicAdd(&ctl->m_r[r], (unsigned long long)filled);
 }
 
 // Hook, over this round's survivor records: a record whose key is the
@@ -943,7 +835,6 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.m = p.m;
     a.n = p.n;
     a.epoch_base = (uint32_t)p.epoch_base;
-    a.cache_max = (uint64_t)ctx->tune_cache_components;
     a.parent = p.parent;
     a.best = p.best;
     a.cand0 = p.cand[0];
@@ -970,10 +861,7 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
     const int vb = vertex_blocks(ctx, a.n);
     {
         KernelScope k(ctx, kKEdgePass);
-        if (ctx->tune_edge_items == 4)
-            edge_pass_kernel<KIND, 4><<<ctx->edge_pass_blocks4, kBlock, pipe_smem<4>(), ctx->stream>>>(a);
-        else
-            edge_pass_kernel<KIND, 8><<<ctx->edge_pass_blocks, kBlock, pipe_smem<8>(), ctx->stream>>>(a);
+        edge_pass_kernel<KIND><<<ctx->edge_pass_blocks, kEpThreads, 0, ctx->stream>>>(a);
     }
     {
         KernelScope k(ctx, kKHook);
@@ -993,16 +881,9 @@ template <int KIND>
 phem_status setup_kernels(phem_context *ctx)
 {
     int per_sm = 0;
-    PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<KIND, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)pipe_smem<8>()));
-    PHEM_CUDA_TRY(cudaFuncSetAttribute(edge_pass_kernel<KIND, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)pipe_smem<4>()));
-    PHEM_CUDA_TRY(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 8>, kBlock, pipe_smem<8>()));
-    ctx->edge_pass_blocks = ctx->sm_count * std::max(1, std::min(per_sm, (int)kMaxEdgeCtasPerSm));
-    PHEM_CUDA_TRY(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND, 4>, kBlock, pipe_smem<4>()));
-    ctx->edge_pass_blocks4 = ctx->sm_count * std::max(1, std::min(per_sm, (int)kMaxEdgeCtasPerSm));
+    PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edge_pass_kernel<KIND>, kEpThreads, 0));
+    const int want = std::min(ctx->tune_edge_ctas, kEpMaxCtasPerSm);
+    ctx->edge_pass_blocks = ctx->sm_count * std::max(1, std::min(per_sm, want));
     PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
     ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
     return PHEM_OK;
@@ -1064,9 +945,13 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
 
 }  // namespace
 
-// Records a survivor list may need: every edge plus one chunk of dead padding
-// per edge-pass CTA (at most kMaxEdgeCtasPerSm per SM).
-uint64_t wl_capacity(uint64_t m, int sm_count) { return m + (uint64_t)sm_count * kMaxEdgeCtasPerSm * kChunk; }
+// Records a survivor list may need: every edge (each flush reserves exactly
+// the records it writes, so a list has no padding).
+uint64_t wl_capacity(uint64_t m, int sm_count)
+{
+    (void)sm_count;
+    return m + 32;
+}
 
 // Workspace of one solve: parent (4n), best (8n), two candidate lists (4n
 // each), the MSF bitmap (m / 8) and two survivor lists (16 bytes per record

@@ -38,6 +38,28 @@ def rmat(scale: int, draws: int, seed: int, abc=RMAT_ABC) -> np.ndarray:
     return out[: m.value]
 
 
+def rmat_range(scale: int, first: int, count: int, seed: int, abc=RMAT_ABC) -> np.ndarray:
+    """Draws [first, first + count) of the rmat() stream, unsorted, in draw order
+    (self-loops dropped): a huge graph batch by batch."""
+    out = np.empty(max(count, 1), np.uint64)
+    m = C.c_uint64()
+    a, b, c = abc
+    check(lib().phem_gen_rmat_range(scale, first, count, a, b, c, seed, out.ctypes.data, C.byref(m)),
+          "phem_gen_rmat_range")
+    return out[: m.value]
+
+
+def rmat_range_device(ctx, scale: int, first: int, count: int, seed: int, out, abc=RMAT_ABC) -> int:
+    """rmat_range on the GPU (libphem's phem_gen_rmat_range_device) into the
+    device tensor `out` (>= count int64 entries); returns the number written."""
+    from ._lib import check as check_phem, lib as phem_lib
+    m = C.c_uint64()
+    a, b, c = abc
+    check_phem(phem_lib().phem_gen_rmat_range_device(ctx.handle, scale, first, count, a, b, c, seed,
+                                                     out.data_ptr(), C.byref(m)), "phem_gen_rmat_range_device")
+    return m.value
+
+
 def weights(m: int, seed: int, bits: int = WEIGHT_BITS) -> np.ndarray:
     w = np.empty(max(m, 1), np.uint32)
     check(lib().phem_gen_weights(m, seed, bits, w.ctypes.data), "phem_gen_weights")

@@ -143,3 +143,18 @@ def test_rmat_range_is_the_same_stream():
         parts.append(out[: m.value])
     got = np.sort(np.concatenate(parts))
     np.testing.assert_array_equal(got, gen.rmat(scale, draws, 9))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scale,first,count", [(16, 0, 1_000_000), (20, 123_457, 777_777), (28, (1 << 33) - 5000, 5000),
+                                               (5, 10, 3)])
+def test_device_rmat_range_equals_host(ctx, scale, first, count):
+    """The GPU generator reproduces the host stream draw for draw (ragged tile
+    counts, a first draw deep into the scale-28 stream, tiny graphs whose draws
+    are mostly self-loops)."""
+    import torch
+    want = gen.rmat_range(scale, first, count, seed=28)
+    out = torch.empty(max(count, 1), dtype=torch.int64, device="cuda")
+    k = gen.rmat_range_device(ctx, scale, first, count, 28, out)
+    assert k == len(want)
+    np.testing.assert_array_equal(out[:k].cpu().numpy().view(np.uint64), want)

@@ -252,38 +252,23 @@ def test_repeated_solves_share_context(ctx):
         assert_msf(ctx.msf_solve(E, g.n), E, ids, cnt, tot)
 
 
-@pytest.mark.parametrize("cache", [0, 1024, 262144])
-def test_offer_cache_setting_does_not_change_the_forest(ctx, cache):
-    """List rounds with and without the per-CTA offer cache give the same
-    forest (hub-heavy R-MAT graph, so the cached rounds do run)."""
-    g = gen.rmat_graph(15, 16, seed=12)
-    E = g.msf_edges()
-    ids, cnt, tot = expect(E, g.n)
-    old = ctx.get_tuning("msf.cache_components")
-    ctx.set_tuning("msf.cache_components", cache)
-    try:
-        r = ctx.msf_solve(E, g.n)
-    finally:
-        ctx.set_tuning("msf.cache_components", old)
-    assert_msf(r, E, ids, cnt, tot)
-
-
-@pytest.mark.parametrize("items", [4, 8])
-def test_edge_items_variants(ctx, items):
-    """Both edge-pass instantiations (4 and 8 records per thread) give the same
-    forest, for weighted and for packed (canonical CC) edges."""
+@pytest.mark.parametrize("ctas", [1, 2, 4])
+def test_edge_pass_grid_sizes(ctx, ctas):
+    """Every edge-pass grid size (warps own different tiles, flush in
+    different orders) gives the same forest, for weighted edges on a hub-heavy
+    R-MAT graph and for packed (canonical CC) edges."""
     g = gen.rmat_graph(15, 16, seed=5)
     E = g.msf_edges()
     ids, cnt, tot = expect(E, g.n)
     c = gen.er_graph(1 << 15, 1 << 17, seed=6)
     labels, forest = oracle.cc_solve(c.pairs, c.n)
-    old = ctx.get_tuning("msf.edge_items")
-    ctx.set_tuning("msf.edge_items", items)
+    old = ctx.get_tuning("msf.edge_ctas_per_sm")
+    ctx.set_tuning("msf.edge_ctas_per_sm", ctas)
     try:
         r = ctx.msf_solve(E, g.n)
         rc = ctx.cc_solve(c.pairs, c.n, canonical=True)
     finally:
-        ctx.set_tuning("msf.edge_items", old)
+        ctx.set_tuning("msf.edge_ctas_per_sm", old)
     assert_msf(r, E, ids, cnt, tot)
     np.testing.assert_array_equal(rc.labels, labels)
     np.testing.assert_array_equal(P.api.forest_set(rc.forest), oracle.forest_set(forest))
