@@ -191,6 +191,27 @@ def cpu_baseline_pbbs(E: np.ndarray, budget_s: float = 20.0, max_runs: int = 5) 
             "seconds_median": med}
 
 
+def bench_reference_gpu(E: np.ndarray, n: int, expect: tuple, runs: int = 3) -> dict:
+    """The reference's own GPU Boruvka (device_boruvka, MST/src/kernels.cu:507-689,
+    built unchanged for sm_100a into oracle/_ref) on the same edges, device
+    resident: CUDA events around the call, median of `runs` after one warm-up,
+    with its forest count and total against ours."""
+    import oracle
+    if not oracle.ref_gpu_available():
+        return {"unavailable": "oracle/_ref/libref_gpu_mst.so was not built (reference tree absent)"}
+    ref = oracle.RefGpuMST(E, n)
+    try:
+        ref.run()
+        out = [ref.run() for _ in range(runs)]
+    finally:
+        ref.close()
+    ms = statistics.median(o[0] for o in out)
+    cnt, tot = out[-1][1], out[-1][2]
+    return {"value": len(E) / (ms / 1e3) / 1e9, "unit": UNIT, "ms": ms, "runs": runs,
+            "count": cnt, "total": tot, "equal_to_ours": (cnt, tot) == tuple(expect),
+            "what": "device_boruvka (MST/src/kernels.cu) on device-resident records, CUDA events around the call"}
+
+
 def bench_cc(ctx, torch, peaks: dict, steps: int, warmup: int, cpu: bool) -> dict:
     """Connected components + spanning forest on Erdos-Renyi n = 2^20 with
     8 * 2^20 uniform draws (seed 1; self-loops dropped, duplicates kept):
@@ -300,8 +321,10 @@ def bench_batched(ctx, torch, num_graphs: int = 4096) -> dict:
     geometric 8-NN (weights floor(distance * 2^24)), every graph solved for
     MSF + labels.  The autotuner picks the kernel configuration, then the
     captured launch is replayed (CUDA events); the one-solve-per-launch path
-    (phem_msf_solve per graph, inputs resident on the host) is timed on a
-    256-graph sample and scaled to the batch by its share of the edges."""
+    is timed on a 256-graph sample, with the inputs on the host
+    (phem_msf_solve per graph) and resident on the device
+    (phem_msf_solve_device per graph), each scaled to the batch by the
+    sample's share of the edges."""
     from phem_graph_b200 import gen
     b = gen.mixed_batch(num_graphs, 4)
     tuned = ctx.batch_autotune(b, reps=2)
@@ -348,6 +371,20 @@ def bench_batched(ctx, torch, num_graphs: int = 4096) -> dict:
     plain_s = time.perf_counter() - t0
     frac = sum(len(e) for e, _ in sample) / b.total_edges
     plain_batch_s = plain_s / frac
+    # the like-for-like baseline: the same sample already resident on the
+    # device, one phem_msf_solve_device call (one launch sequence) per graph
+    d_sample = [(torch.from_numpy(e.view(np.int32)).to(dev), len(e), n) for e, n in sample]
+    d_out = torch.empty((max(n for _, _, n in d_sample), 3), dtype=torch.int32, device=dev)
+    d_ct = torch.zeros(2, dtype=torch.int64, device=dev)
+    for d_e, m_g, n_g in d_sample[:8]:
+        ctx.msf_solve_device(d_e, m_g, n_g, d_out, d_ct)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for d_e, m_g, n_g in d_sample:
+        ctx.msf_solve_device(d_e, m_g, n_g, d_out, d_ct)
+    torch.cuda.synchronize()
+    dev_batch_s = (time.perf_counter() - t0) / frac
+    del d_sample, d_out
     return {"workload": "batched_4096_mixed_er_rgg", "graphs": b.num_graphs, "edges": b.total_edges,
             "vertices": b.total_vertices, "unit": UNIT, "value": b.total_edges / (ms / 1e3) / 1e9,
             "ms_per_batch": ms, "graphs_per_s": b.num_graphs / (ms / 1e3), "launches_per_batch": 1,
@@ -356,25 +393,23 @@ def bench_batched(ctx, torch, num_graphs: int = 4096) -> dict:
             "one_launch_per_graph": {"value": b.total_edges / plain_batch_s / 1e9, "s_per_batch": plain_batch_s,
                                      "sample": "256 graphs through phem_msf_solve, scaled by edge share"},
             "speedup_vs_one_launch_per_graph": plain_batch_s / (ms / 1e3),
+            "one_launch_per_graph_device": {"value": b.total_edges / dev_batch_s / 1e9, "s_per_batch": dev_batch_s,
+                                            "sample": "the same 256 graphs resident on the device, one "
+                                                      "phem_msf_solve_device per graph, scaled by edge share; "
+                                                      "that path waits on the host between round batches, so "
+                                                      "it has no captured form"},
+            "speedup_vs_one_launch_per_graph_device": dev_batch_s / (ms / 1e3),
             "e2e": {"value": b.total_edges / e2e / 1e9, "unit": UNIT, "ms_per_step": e2e * 1e3,
                     "h2d_bytes_per_step": 12 * b.total_edges + 24 * b.num_graphs,
                     "d2h_bytes_per_step": 8 * b.total_vertices + 12 * b.num_graphs,
                     "api": "phem_batch_solve (C ABI), pinned host edges and results, median of 3"}}
 
 
-def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), per_rate: int = 256) -> dict:
-    """Served request stream: Poisson arrivals at each rate, requests drawn
-    from a pool of 64 graphs with m log-uniform in [2^10, 2^24] (70% CC packed
-    pairs, 30% MSF records with weights U[1, 2^20]; half Erdos-Renyi, half
-    R-MAT), request buffers in pinned host memory, a 64 GB device budget.
-    Latency = submission to result written to host; throughput = edges of all
-    requests / wall time of the run.  The serial baseline solves the same
-    pool one request at a time through the one-graph entry points."""
-    import phem_graph_b200 as P
-    from phem_graph_b200.serve import PHEM_BATCH_MSF, Server, poisson_arrivals, request_pool
-    pool = request_pool(64, seed=5)
-    keep = []
-    for g in pool:  # pinned request buffers, as a server's receive path would hold them
+def _pin_pool(torch, pool, keep):
+    """Moves every request buffer of a pool to pinned host memory (a server's
+    receive path would hold them that way)."""
+    from phem_graph_b200.serve import PHEM_BATCH_MSF
+    for g in pool:
         if g.kind == PHEM_BATCH_MSF:
             t = torch.from_numpy(g.edges.view(np.int32)).pin_memory()
             keep.append(t)
@@ -383,6 +418,17 @@ def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), per_rate: int 
             t = torch.from_numpy(g.pairs.view(np.int64)).pin_memory()
             keep.append(t)
             g.pairs = t.numpy().view(np.uint64)
+
+
+def _served_stream(torch, srv, pool, rates, requests: int, rng, h2d_gbs: float) -> dict:
+    """One request stream through the server at every offered rate: achieved
+    vs offered req/s, p50 / p99 latency (submission to result in host memory),
+    throughput, the share of requests on the batched path and the host-link
+    fraction (request bytes in + result bytes out over the wall time, against
+    a plain pinned copy).  A rate is sustained when the server achieved >= 95 %
+    of it; latencies at unsustained rates measure queue growth, not service."""
+    import phem_graph_b200 as P
+    from phem_graph_b200.serve import PHEM_BATCH_MSF, poisson_arrivals
     ctx = P.Context(0)
     solve = (lambda g: ctx.msf_solve(g.edges, g.n) if g.kind == PHEM_BATCH_MSF
              else ctx.cc_solve(g.pairs, g.n, want_forest=False))
@@ -394,33 +440,76 @@ def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), per_rate: int 
     serial_s = time.perf_counter() - t0
     ctx.close()
     pool_edges = sum(g.m for g in pool)
-    rng = np.random.default_rng(1)
+    serial = {"value": pool_edges / serial_s / 1e9, "req_s": len(pool) / serial_s,
+              "api": "phem_msf_solve / phem_cc_solve one request at a time (one solve per launch sequence), "
+                     "pinned host inputs, host results"}
+    srv.replay(pool, np.zeros(len(pool), np.uint64))  # warm-up: every worker sizes its workspace
     points = []
+    for rate in rates:
+        idx = rng.integers(0, len(pool), requests)
+        reqs = [pool[i] for i in idx]
+        arr = poisson_arrivals(requests, rate, seed=rate)
+        t0 = time.perf_counter()
+        res = srv.replay(reqs, arr)
+        wall = time.perf_counter() - t0
+        assert all(r.status == 0 for r in res)
+        lat = np.array([r.latency_ns for r in res]) / 1e6
+        e = sum(g.m for g in reqs)
+        io = sum((g.m * 12 + 12 * max(g.n - 1, 1)) if g.kind == PHEM_BATCH_MSF else (g.m * 8 + 4 * g.n)
+                 for g in reqs)
+        achieved = requests / wall
+        points.append({"rate_req_s": rate, "requests": requests, "seconds": wall, "req_s": achieved,
+                       "sustained": achieved >= 0.95 * rate, "p50_ms": float(np.percentile(lat, 50)),
+                       "p99_ms": float(np.percentile(lat, 99)), "throughput": e / wall / 1e9,
+                       "batched_share": float(np.mean([r.path == 0 for r in res])),
+                       "host_link_frac": io / wall / 1e9 / h2d_gbs})
+    sus = [p for p in points if p["sustained"]]
+    best = max(points, key=lambda p: p["throughput"])
+    return {"points": points, "value": best["throughput"], "serial_plain": serial,
+            "speedup_vs_serial_plain": best["throughput"] / serial["value"],
+            "saturation_req_s": max(p["req_s"] for p in points),
+            "knee_rate_req_s": max((p["rate_req_s"] for p in sus), default=None),
+            "latency_at_knee": ({"p50_ms": sus[-1]["p50_ms"], "p99_ms": sus[-1]["p99_ms"]} if sus else None),
+            "pool_graphs": len(pool), "pool_edges": pool_edges}
+
+
+def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), requests: int = 2000) -> dict:
+    """Served request streams (Poisson arrivals at each offered rate, 2000
+    requests per rate, a 64 GB device budget, request buffers in pinned host
+    memory):
+      mixed  -- the configured stream: m log-uniform in [2^10, 2^24], 70% CC
+                packed pairs / 30% MSF records (weights U[1, 2^20]), half
+                Erdos-Renyi, half R-MAT (a pool of 64 graphs);
+      small  -- the same stream limited to m <= 2^18 (the server's batched
+                path; a pool of 256 graphs), the small-graph case whose
+                throughput the target compares with one solve per launch.
+    Each stream is compared with its own pool solved one request at a time
+    through the one-graph entry points."""
+    from phem_graph_b200.serve import Server, request_pool
+    keep = []
+    mixed = request_pool(64, seed=5)
+    small = request_pool(256, seed=6, m_hi=1 << 18)
+    _pin_pool(torch, mixed, keep)
+    _pin_pool(torch, small, keep)
+    # host link: one pinned copy of 256 MB
+    h = torch.empty(1 << 25, dtype=torch.int64, pin_memory=True)
+    d = torch.empty(1 << 25, dtype=torch.int64, device="cuda")
+    d.copy_(h, non_blocking=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d.copy_(h, non_blocking=True)
+    torch.cuda.synchronize()
+    h2d_gbs = 8 * (1 << 25) / (time.perf_counter() - t0) / 1e9
+    del h, d
+    rng = np.random.default_rng(1)
+    cfg = {"memory_budget_gb": 64, "slots": 2, "max_batch_graphs": 1024, "large_edges": 1 << 18,
+           "large_workers": 2, "requests_per_rate": requests, "h2d_gbs": h2d_gbs}
     with Server(memory_budget=64 << 30, slots=2, max_batch_graphs=1024, large_edges=1 << 18,
                 large_workers=2) as srv:
-        srv.replay(pool, np.zeros(len(pool), np.uint64))  # warm-up: every worker sizes its workspace
-        # and a short paced run, so the first measured rate starts from the
-        # same steady state as the others
-        srv.replay([pool[i] for i in rng.integers(0, len(pool), 64)], poisson_arrivals(64, rates[0], seed=7))
-        for rate in rates:
-            reqs = [pool[i] for i in rng.integers(0, len(pool), per_rate)]
-            arr = poisson_arrivals(per_rate, rate, seed=rate)
-            t0 = time.perf_counter()
-            res = srv.replay(reqs, arr)
-            wall = time.perf_counter() - t0
-            lat = np.array([s.latency_ns for s in res]) / 1e6
-            assert all(s.status == 0 for s in res)
-            e = sum(g.m for g in reqs)
-            points.append({"rate_req_s": rate, "requests": per_rate, "p50_ms": float(np.percentile(lat, 50)),
-                           "p99_ms": float(np.percentile(lat, 99)), "throughput": e / wall / 1e9,
-                           "req_s": per_rate / wall,
-                           "batched_share": float(np.mean([s.path == 0 for s in res]))})
-    return {"workload": "served_poisson_m_loguniform_2^10_2^24_70cc_30msf", "unit": UNIT, "points": points,
-            "value": max(p["throughput"] for p in points),
-            "serial_plain": {"value": pool_edges / serial_s / 1e9, "req_s": len(pool) / serial_s,
-                             "api": "phem_msf_solve / phem_cc_solve one request at a time, pinned host inputs"},
-            "config": {"memory_budget_gb": 64, "slots": 2, "max_batch_graphs": 1024, "large_edges": 1 << 18,
-                       "large_workers": 2, "pool_graphs": len(pool), "pool_edges": pool_edges}}
+        out_mixed = _served_stream(torch, srv, mixed, rates, requests, rng, h2d_gbs)
+        out_small = _served_stream(torch, srv, small, rates, requests, rng, h2d_gbs)
+    return {"workload": "served_poisson_m_loguniform_2^10_2^24_70cc_30msf", "unit": UNIT,
+            "value": out_mixed["value"], "mixed": out_mixed, "small": out_small, "config": cfg}
 
 
 def bench_streamed(ctx, torch, scale: int, edge_factor: int = 32, batch: int = 1 << 28, cpu: bool = True) -> dict:
@@ -722,8 +811,21 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import tempfile
+
     import oracle
-    g, E = rmat22(0, args.scale, args.edge_factor)
+    # The input is generated in a child process (phem_graph_b200.gen, host
+    # code of this build) and handed over as a file, so this process maps the
+    # reference's libraries only.
+    with tempfile.TemporaryDirectory() as tmp:
+        f = os.path.join(tmp, "edges.npy")
+        code = ("import sys, numpy as np; sys.path.insert(0, sys.argv[1]); from phem_graph_b200 import gen; "
+                "g = gen.rmat_graph(int(sys.argv[2]), int(sys.argv[3]), seed=22); "
+                "np.save(sys.argv[4], g.msf_edges()); print(g.n)")
+        out = subprocess.run([sys.executable, "-c", code, str(ROOT), str(args.scale), str(args.edge_factor), f],
+                             check=True, capture_output=True, text=True).stdout
+        E = np.load(f)
+    n = int(out.split()[-1])
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference tree absent)"}))
         return
@@ -733,15 +835,16 @@ def run_reference(args) -> None:
     times = [ref.run() for _ in range(args.steps)]
     workers = ref.workers()
     total = sum(times)
-    value = args.steps * g.m / total / 1e9
+    m = len(E)
+    value = args.steps * m / total / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"msf_rmat{args.scale}_ef{args.edge_factor}", "n": g.n, "m": g.m, "seed": 22,
+        "config": {"workload": f"msf_rmat{args.scale}_ef{args.edge_factor}", "n": n, "m": m, "seed": 22,
                    "weights": "uniform [1, 2^20]"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "reference",
-                         "sample": f"PBBS mst() on the full {g.m}-edge array, {args.steps} timed runs"},
+                         "sample": f"PBBS mst() on the full {m}-edge array, {args.steps} timed runs"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -938,6 +1041,11 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_extra:
         # the other workloads of the metric, measured after the headline run
         del d_edges, d_out
+        torch.cuda.empty_cache()
+        try:
+            line["reference_gpu"] = bench_reference_gpu(E, n, (stats.count, stats.total))
+        except RuntimeError as e:
+            line["reference_gpu"] = {"error": str(e)[:300]}
         torch.cuda.empty_cache()
         line["csr_input"] = bench_csr_input(ctx, torch, g, max(3, args.steps // 2), args.warmup,
                                             (stats.count, stats.total))

@@ -200,6 +200,13 @@ def _ref_lib(name: str) -> C.CDLL:
             L.ref_cc_reset.argtypes = [C.c_void_p]
             L.ref_cc_get.argtypes = [C.c_void_p, _i32p, _u64p]
             L.ref_cc_workers.restype = C.c_int32
+        elif name == "libref_gpu_mst.so":
+            L.ref_gpu_mst_create.argtypes = [_u32p, C.c_uint64, C.c_uint32]
+            L.ref_gpu_mst_create.restype = C.c_void_p
+            L.ref_gpu_mst_run.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint64),
+                                          C.POINTER(C.c_uint64)]
+            L.ref_gpu_mst_run.restype = C.c_int
+            L.ref_gpu_mst_destroy.argtypes = [C.c_void_p]
         elif name == "libref_mst.so":
             L.ref_mst_create.argtypes = [_u32p, C.c_uint64]
             L.ref_mst_create.restype = C.c_void_p
@@ -255,6 +262,40 @@ class RefCC:
             self.close()
         except Exception:
             pass
+
+
+class RefGpuMST:
+    """The reference's GPU Boruvka device_boruvka (MST/src/kernels.cu:507-689),
+    built for sm_100a: device copies of the edges made once, each run() times
+    the call alone with CUDA events on fresh copies; returns (ms, count, total)."""
+
+    def __init__(self, E, n: int):
+        self.L = _ref_lib("libref_gpu_mst.so")
+        E = _edges3(E)
+        self.h = self.L.ref_gpu_mst_create(E.reshape(-1), len(E), n)
+        if not self.h:
+            raise RuntimeError("ref_gpu_mst_create failed (device memory)")
+
+    def run(self):
+        ms, cnt, tot = C.c_float(), C.c_uint64(), C.c_uint64()
+        if self.L.ref_gpu_mst_run(self.h, C.byref(ms), C.byref(cnt), C.byref(tot)) != 0:
+            raise RuntimeError("device_boruvka failed")
+        return float(ms.value), int(cnt.value), int(tot.value)
+
+    def close(self) -> None:
+        if self.h:
+            self.L.ref_gpu_mst_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_gpu_available() -> bool:
+    return (REF_DIR / "libref_gpu_mst.so").exists()
 
 
 class RefPBBS:

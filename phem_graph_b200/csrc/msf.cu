@@ -62,6 +62,7 @@ struct RoundArgs {
     uint64_t *status;
     unsigned long long *forest;
     Ctl *ctl;
+    uint64_t light_k;  // light edges the threshold aims at (sizes the edge pass's list chunks)
 };
 
 // An input record takes part in the forest: self-loops never do; packed CC
@@ -81,15 +82,41 @@ __device__ __forceinline__ unsigned long long e0_key(uint32_t w, uint64_t id)
     return KIND == kKindMsf ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
 }
 
+// Per-CTA pre-reduction of offers.  Most survivors of hub-heavy rounds (and
+// the heavy pass, whose records mostly touch the light phase's giant
+// component) offer to a handful of roots, and atomics on one best[] word
+// serialise on its L2 slice.  A root claims the slot hash(t) of a 512-entry
+// table in shared memory on its first offer; offers to a claimed slot are
+// shared-memory atomicMins, offers that collide with another root go to
+// best[] directly, and the table is flushed to best[] (one atomic per slot)
+// when the CTA's pass ends.  Shared: tags 2 KB, keys 4 KB.
+constexpr int kOfferSlots = 512;
+constexpr uint32_t kNoTag = 0xffffffffu;
+
+struct OfferCache {
+    unsigned long long key[kOfferSlots];
+    uint32_t tag[kOfferSlots];
+};
+
+__device__ __forceinline__ void offer_one(unsigned long long *best, OfferCache &oc, uint32_t t,
+                                          unsigned long long k)
+{
+    const int slot = (int)((t * 0x9E3779B1u) >> 23);  // 9 bits
+    uint32_t tag = *(volatile uint32_t *)&oc.tag[slot];
+    if (tag == kNoTag)
+        tag = atomicCAS(&oc.tag[slot], kNoTag, t);
+    if (tag == kNoTag || tag == t)
+        atomicMin(&oc.key[slot], k);
+    else
+        atomicMin(best + t, k);  // fire and forget: no guard read on the warp's path
+}
+
 // Offers `key` to best[ta] and best[tb] for the live lanes of a warp.  Lanes
 // with the same target are grouped (__match_any_sync) and their keys reduced
 // (high word, then low word among the lanes holding the minimum high word)
-// so each group does one atomic: a hub's records arrive in runs.  The group
-// leader reads best[t] first and skips the atomic when its key cannot win;
-// the read may be stale but is never below the true value.  Both targets'
-// guard reads are issued before either atomic.  Fire-and-forget 64-bit
-// atomicMin; every lane of the warp calls this, converged.
-__device__ __forceinline__ void offer_pair(unsigned long long *best, uint32_t ta, uint32_t tb,
+// so each group makes one offer: a hub's records arrive in runs.  Every lane
+// of the warp calls this, converged.
+__device__ __forceinline__ void offer_pair(unsigned long long *best, OfferCache &oc, uint32_t ta, uint32_t tb,
                                            unsigned long long key, bool on)
 {
     const unsigned act = __ballot_sync(0xffffffffu, on);
@@ -102,14 +129,10 @@ __device__ __forceinline__ void offer_pair(unsigned long long *best, uint32_t ta
     const uint32_t alo = __reduce_min_sync(pa, hi == ahi ? lo : 0xffffffffu);
     const uint32_t blo = __reduce_min_sync(pb, hi == bhi ? lo : 0xffffffffu);
     const uint32_t lane = lane_id();
-    const bool la = (int)lane == __ffs(pa) - 1, lb = (int)lane == __ffs(pb) - 1;
-    const unsigned long long ka = ((unsigned long long)ahi << 32) | alo, kb = ((unsigned long long)bhi << 32) | blo;
-    const unsigned long long ga = la ? __ldcg(best + ta) : 0ull;
-    const unsigned long long gb = lb ? __ldcg(best + tb) : 0ull;
-    if (la && ka < ga)
-        atomicMin(best + ta, ka);
-    if (lb && kb < gb)
-        atomicMin(best + tb, kb);
+    if ((int)lane == __ffs(pa) - 1)
+        offer_one(best, oc, ta, ((unsigned long long)ahi << 32) | alo);
+    if ((int)lane == __ffs(pb) - 1)
+        offer_one(best, oc, tb, ((unsigned long long)bhi << 32) | blo);
 }
 
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
@@ -276,24 +299,83 @@ __device__ __forceinline__ void ring_append(EpWarp &w, uint32_t &filled, bool ke
     filled += __popc(mask);
 }
 
+// List space of one CTA.  Warps take exact slot ranges from the CTA's current
+// chunk (a shared-memory atomic); the warp whose request crosses the chunk's
+// end takes the chunk's last slots plus the start of the next chunk, which it
+// reserves with one global atomicAdd and publishes; warps that arrive
+// meanwhile wait for the new chunk.  One global atomic per chunk, not per
+// flush: a single list counter takes about one returning atomic per few
+// clocks, which per-flush reservations (10 M survivors / 32) saturated.
+// Chunks are taken lazily, so a CTA without survivors reserves nothing; the
+// CTA's last chunk is padded with dead records {0, 0, 0, 0} (equal roots:
+// the next pass drops them) when the pass ends.
+struct EpChunks {
+    unsigned long long state;    // (chunk number << 32) | slots handed out in it
+    unsigned long long base[8];  // list index of chunk c at [c & 7]
+    uint32_t size;               // records per chunk
+};
+
+// Slots of one request: [b1, b1 + split) then [b2, b2 + k - split).
+struct EpSlots {
+    unsigned long long b1, b2;
+    uint32_t split;
+};
+
+// Reserves k (1..32) list slots; split = 0 and b1 = ~0 when a wait for a new
+// chunk gave up (the status bit is set).  Lane 0 only.
+__device__ __noinline__ EpSlots chunk_reserve(EpChunks &c, unsigned long long *len, uint32_t k, uint32_t *err)
+{
+    const uint32_t C = c.size;
+    for (uint32_t spins = 0; spins < kMbarSpinCap; spins++) {
+        const unsigned long long old = atomicAdd(&c.state, (unsigned long long)k);
+        __threadfence_block();
+        const uint32_t cid = (uint32_t)(old >> 32), used = (uint32_t)old;
+        if (used + k <= C) {
+            const unsigned long long b = *(volatile unsigned long long *)&c.base[cid & 7] + used;
+            return EpSlots{b, b, k};
+        }
+        if (used <= C) {
+            // this request closes chunk cid (its last C - used slots; none for
+            // the empty chunk 0) and opens chunk cid + 1 with the rest
+            const uint32_t split = cid > 0 ? C - used : 0;
+            const unsigned long long b1 = cid > 0 ? *(volatile unsigned long long *)&c.base[cid & 7] + used : 0;
+            const unsigned long long nb = atomicAdd(len, (unsigned long long)C);
+            *(volatile unsigned long long *)&c.base[(cid + 1) & 7] = nb;
+            __threadfence_block();
+            atomicExch(&c.state, ((unsigned long long)(cid + 1) << 32) | (k - split));
+            return EpSlots{b1, nb, split};
+        }
+        // another warp is opening the next chunk
+        while ((uint32_t)(*(volatile unsigned long long *)&c.state >> 32) == cid)
+            if (++spins >= kMbarSpinCap)
+                break;
+    }
+    set_err(err, kErrLookback);
+    return EpSlots{~0ull, ~0ull, 0};
+}
+
 // Writes the `cnt` (<= 32) oldest ring entries to the list and offers them.
 template <int KIND>
-__device__ __forceinline__ void ring_flush(const RoundArgs &a, uint4 *out, unsigned long long *len, EpWarp &w,
-                                           uint32_t &flushed, uint32_t cnt, uint32_t lane)
+__device__ __forceinline__ void ring_flush(const RoundArgs &a, uint4 *out, unsigned long long *len, EpChunks &ch,
+                                           OfferCache &oc, EpWarp &w, uint32_t &flushed, uint32_t cnt,
+                                           uint32_t lane)
 {
     __syncwarp();  // the lanes' ring writes are visible
     const bool on = lane < cnt;
     const uint4 rec = on ? w.ring[(flushed + lane) & (kRing - 1)] : make_uint4(0, 0, 0, 0);
     flushed += cnt;
-    unsigned long long base = 0;
+    EpSlots sl{0, 0, 0};
     if (lane == 0)
-        base = atomicAdd(len, (unsigned long long)cnt);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (on)
-        out[base + lane] = rec;
-    const unsigned long long key =
-        KIND == kKindMsf ? (((unsigned long long)rec.z << 32) | rec.w) : (unsigned long long)rec.w;
-    offer_pair(a.best, rec.x, rec.y, key, on);
+        sl = chunk_reserve(ch, len, cnt, &a.ctl->err);
+    const unsigned long long b1 = __shfl_sync(0xffffffffu, sl.b1, 0), b2 = __shfl_sync(0xffffffffu, sl.b2, 0);
+    const uint32_t split = __shfl_sync(0xffffffffu, sl.split, 0);
+    if (b2 != ~0ull) {
+        if (on)
+            out[lane < split ? b1 + lane : b2 + (lane - split)] = rec;
+        const unsigned long long key =
+            KIND == kKindMsf ? (((unsigned long long)rec.z << 32) | rec.w) : (unsigned long long)rec.w;
+        offer_pair(a.best, oc, rec.x, rec.y, key, on);
+    }
     __syncwarp();  // the ring slots just read may be written again
 }
 
@@ -313,7 +395,8 @@ template <int KIND, bool LIGHT>
 __device__ __forceinline__ void ep_input_tile(const RoundArgs &a, const unsigned char *stage, bool bulk,
                                               uint64_t tbase, uint32_t rem, uint32_t thr_hi, uint32_t thr_lo,
                                               EpWarp &w, uint32_t &filled, uint32_t &flushed, uint4 *out,
-                                              unsigned long long *len, uint32_t lane, bool &any_bad)
+                                              unsigned long long *len, EpChunks &ch, OfferCache &oc,
+                                              uint32_t lane, bool &any_bad)
 {
     constexpr uint32_t REC = KIND == kKindMsf ? 12u : 8u;
     constexpr int ROWS = (int)(ep_tile_recs<REC>() / 32);
@@ -374,7 +457,7 @@ __device__ __forceinline__ void ep_input_tile(const RoundArgs &a, const unsigned
     for (int j = 0; j < ROWS; j++) {
         ring_append(w, filled, keep[j], make_uint4(u[j], v[j], wt[j], id0 + j * 32 + lane), lane);
         if (filled - flushed >= 32)
-            ring_flush<KIND>(a, out, len, w, flushed, 32, lane);
+            ring_flush<KIND>(a, out, len, ch, oc, w, flushed, 32, lane);
     }
 }
 
@@ -384,7 +467,8 @@ __device__ __forceinline__ void ep_input_tile(const RoundArgs &a, const unsigned
 template <int KIND>
 __device__ __forceinline__ void ep_list_tile(const RoundArgs &a, const uint4 *in, const unsigned char *stage,
                                              bool bulk, uint64_t tbase, uint32_t rem, EpWarp &w, uint32_t &filled,
-                                             uint32_t &flushed, uint4 *out, unsigned long long *len, uint32_t lane)
+                                             uint32_t &flushed, uint4 *out, unsigned long long *len, EpChunks &ch,
+                                             OfferCache &oc, uint32_t lane)
 {
     constexpr int ROWS = (int)(ep_tile_recs<16>() / 32);
     uint4 rec[ROWS];
@@ -409,7 +493,7 @@ __device__ __forceinline__ void ep_list_tile(const RoundArgs &a, const uint4 *in
     for (int j = 0; j < ROWS; j++) {
         ring_append(w, filled, keep[j] && rec[j].x != rec[j].y, rec[j], lane);
         if (filled - flushed >= 32)
-            ring_flush<KIND>(a, out, len, w, flushed, 32, lane);
+            ring_flush<KIND>(a, out, len, ch, oc, w, flushed, 32, lane);
     }
 }
 
@@ -417,6 +501,8 @@ template <int KIND>
 __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(RoundArgs a)
 {
     __shared__ EpWarp s_warp[kEpWarps];
+    __shared__ EpChunks s_chunks;
+    __shared__ OfferCache s_offers;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
@@ -438,6 +524,24 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
     const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
     const uint32_t thr_hi = (uint32_t)(thr >> 32), thr_lo = (uint32_t)thr;
     const uint64_t policy = l2_evict_first();  // inputs and lists are read once per pass
+    if (threadIdx.x == 0) {
+        // chunks of about 1/16 of a CTA's expected survivors (a power of two
+        // in [64, 2048]): few global atomics, and on average half a chunk of
+        // padding per CTA.  Expected: the light edges in round 0, an eighth of
+        // the input in the heavy pass, the whole list in list rounds.
+        const uint64_t expect = src == kSrcLight ? a.light_k : (src == kSrcHeavy ? a.m / 8 : count);
+        const uint64_t per = expect / ((uint64_t)gridDim.x * 16);
+        uint32_t c = 64;
+        while (c < 2048 && (uint64_t)c * 2 <= per)
+            c *= 2;
+        s_chunks.size = c;
+        s_chunks.state = (unsigned long long)c;  // chunk 0 "full": the first request opens chunk 1
+    }
+    for (int i = threadIdx.x; i < kOfferSlots; i += kEpThreads) {
+        s_offers.tag[i] = kNoTag;
+        s_offers.key[i] = kKeyNone;
+    }
+    __syncthreads();
 
     if (lane == 0) {
         for (int s = 0; s < kEpStages; s++)
@@ -480,30 +584,43 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
         const uint64_t left = count - tbase;
         const uint32_t rem = left < tile_recs ? (uint32_t)left : tile_recs;
         if (src == kSrcList)
-            ep_list_tile<KIND>(a, in, w.stage[s], bulk, tbase, rem, w, filled, flushed, out, len, lane);
+            ep_list_tile<KIND>(a, in, w.stage[s], bulk, tbase, rem, w, filled, flushed, out, len, s_chunks,
+                               s_offers, lane);
         else if (src == kSrcLight)
             ep_input_tile<KIND, true>(a, w.stage[s], bulk, tbase, rem, thr_hi, thr_lo, w, filled, flushed, out,
-                                      len, lane, any_bad);
+                                      len, s_chunks, s_offers, lane, any_bad);
         else
             ep_input_tile<KIND, false>(a, w.stage[s], bulk, tbase, rem, thr_hi, thr_lo, w, filled, flushed, out,
-                                       len, lane, any_bad);
+                                       len, s_chunks, s_offers, lane, any_bad);
         fence_proxy_async_smem();  // this lane's reads of the stage precede its refill
         __syncwarp();
     }
     if (failed) {
         // a copy never completed (the status bit is set): wait, bounded, for
-        // every copy still in flight into this warp's stages before leaving
+        // every copy still in flight into this warp's stages
         for (int q = 0; q < kEpStages; q++)
             if (pending & (1u << q))
                 ep_wait(&w.bar[q], (parity >> q) & 1u, &ctl->err);
-        return;
+    } else {
+        if (filled != flushed)
+            ring_flush<KIND>(a, out, len, s_chunks, s_offers, w, flushed, filled - flushed, lane);
+        if (__any_sync(0xffffffffu, any_bad) && lane == 0 && src == kSrcLight)
+            set_err(&ctl->err, kErrRange);
+        if (lane == 0 && filled)
+            atomicAdd(&ctl->m_r[r], (unsigned long long)filled);
     }
-    if (filled != flushed)
-        ring_flush<KIND>(a, out, len, w, flushed, filled - flushed, lane);
-    if (__any_sync(0xffffffffu, any_bad) && lane == 0 && src == kSrcLight)
-        set_err(&ctl->err, kErrRange);
-    if (lane == 0 && filled)
-        atomicAdd(&ctl->m_r[r], (unsigned long long)filled);
+    // the CTA's last chunk: pad its unused tail; the offer table goes to best[]
+    __syncthreads();
+    for (int i = threadIdx.x; i < kOfferSlots; i += kEpThreads) {
+        const uint32_t t = s_offers.tag[i];
+        if (t != kNoTag)
+            atomicMin(a.best + t, s_offers.key[i]);
+    }
+    const unsigned long long st = s_chunks.state;
+    const uint32_t cid = (uint32_t)(st >> 32), used = min((uint32_t)st, s_chunks.size);
+    if (cid > 0)
+        for (uint32_t i = used + threadIdx.x; i < s_chunks.size; i += kEpThreads)
+            out[s_chunks.base[cid & 7] + i] = make_uint4(0, 0, 0, 0);
 }
 
 // Hook, over this round's survivor records: a record whose key is the
@@ -517,14 +634,14 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
 {
-    __shared__ unsigned long long s_red[kWarps];
+    __shared__ uint32_t s_warp[kWarps + 1];
+    __shared__ unsigned long long s_base;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const uint64_t len = ctl->wl_len[r];
     const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
-    unsigned long long chosen = 0;
     const uint64_t step = (uint64_t)gridDim.x * kBlock * 4;
     for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * 4; i0 < len; i0 += step) {
         uint4 rec[4];
@@ -539,6 +656,7 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
             ka[q] = real ? __ldg(a.best + rec[q].x) : 0ull;
             kb[q] = real ? __ldg(a.best + rec[q].y) : 0ull;
         }
+        uint32_t choosers = 0;  // bit 2q: rec q chosen by its first root, 2q + 1: by its second
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             if (rec[q].x == rec[q].y)
@@ -547,7 +665,7 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
             const bool A = ka[q] == key, B = kb[q] == key;
             if (!A && !B)
                 continue;
-            chosen += (unsigned long long)A + (unsigned long long)B;
+            choosers |= ((uint32_t)A << (2 * q)) | ((uint32_t)B << (2 * q + 1));
             uint32_t hk, tgt;
             if (A && B) {
                 hk = rec[q].x > rec[q].y ? rec[q].x : rec[q].y;
@@ -565,55 +683,61 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
             if (KIND == kKindPacked && a.forest)
                 a.forest[hk] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
         }
+        // the round's choosers (each component finds its one record) go to
+        // the chooser list, which the compress walks instead of all vertices
+        uint32_t total;
+        uint32_t off = block_exclusive_scan(__popc(choosers), &total, s_warp);
+        if (total == 0)
+            continue;  // uniform
+        if (threadIdx.x == 0)
+            s_base = atomicAdd(&ctl->n_r[r], (unsigned long long)total);
+        __syncthreads();
+        const unsigned long long base = s_base;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (choosers & (1u << (2 * q)))
+                a.cand0[base + off++] = rec[q].x;
+            if (choosers & (1u << (2 * q + 1)))
+                a.cand0[base + off++] = rec[q].y;
+        }
+        __syncthreads();  // s_warp and s_base are reused
     }
-    const unsigned long long tot = block_sum_u64(chosen, s_red);
-    if (threadIdx.x == 0 && tot)
-        atomicAdd(&ctl->n_r[r], tot);
 }
 
 constexpr int kVItems = 4;  // candidates per thread per iteration of the vertex kernels
 
-// Pointer jumping.  Normally over this round's components only: roots that
-// remain are collected as the next round's candidates (one atomicAdd per
-// block-iteration) and best is reset.  In the round where the light phase runs
-// dry every vertex is compressed to its root instead, so the heavy pass
-// relabels original endpoints in one hop.
+// Pointer jumping over this round's choosers (the hook's list): each is
+// pointed at its root and its best key is reset.  In the round where the
+// light phase runs dry (no survivors, no choosers) every vertex is compressed
+// to its root instead, so the heavy pass relabels original endpoints in one
+// hop.
 __device__ void advance_round(Ctl *ctl);
 
 __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
 {
-    __shared__ uint32_t s_warp[kWarps];
-    __shared__ uint32_t s_base;
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
-    const bool all = *(volatile uint32_t *)&ctl->cand_all;
     const bool full = *(volatile uint32_t *)&ctl->phase == 0 && ctl->m_r[r] == 0;
-    const uint64_t count = (all || full) ? a.n : ctl->roots[r];
-    const uint32_t *cand = (r & 1) ? a.cand1 : a.cand0;
-    uint32_t *next = (r & 1) ? a.cand0 : a.cand1;
-    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint64_t count = full ? a.n : ctl->n_r[r];
     const uint64_t step = (uint64_t)gridDim.x * kBlock * kVItems;
     for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * kVItems; i0 < count; i0 += step) {
-        bool stays[kVItems], active[kVItems], walking[kVItems];
+        bool walking[kVItems];
         uint32_t x[kVItems], y[kVItems], y0[kVItems];
         // the candidates' loads and root walks advance in lockstep, so their
         // dependent loads are in flight together
 #pragma unroll
         for (int k = 0; k < kVItems; k++) {
             const uint64_t i = i0 + k * kBlock + threadIdx.x;
-            active[k] = i < count;
-            x[k] = active[k] ? ((all || full) ? (uint32_t)i : cand[i]) : 0;
+            walking[k] = i < count;
+            x[k] = walking[k] ? (full ? (uint32_t)i : __ldcg(a.cand0 + i)) : 0;
         }
 #pragma unroll
         for (int k = 0; k < kVItems; k++)
-            active[k] = active[k] && (full || a.best[x[k]] != kKeyNone);
-#pragma unroll
-        for (int k = 0; k < kVItems; k++) {
-            y0[k] = y[k] = active[k] ? a.parent[x[k]] : x[k];
-            walking[k] = active[k];
-        }
+            y0[k] = y[k] = walking[k] ? a.parent[x[k]] : x[k];
+        const bool active[kVItems] = {walking[0], walking[1], walking[2], walking[3]};
+        static_assert(kVItems == 4, "active[] lists kVItems entries");
         for (uint32_t steps = 0;; steps++) {
             uint32_t p[kVItems];
 #pragma unroll
@@ -635,46 +759,13 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
         }
 #pragma unroll
         for (int k = 0; k < kVItems; k++) {
-            stays[k] = false;
             if (active[k]) {
                 if (y0[k] != y[k])
                     a.parent[x[k]] = y[k];
-                if (!full) {
+                if (!full)
                     a.best[x[k]] = kKeyNone;
-                    stays[k] = (y[k] == x[k]);
-                }
             }
         }
-        if (full)
-            continue;  // uniform: no candidate list in the compress-all round
-        unsigned m[kVItems];
-        uint32_t wsum = 0;
-#pragma unroll
-        for (int k = 0; k < kVItems; k++) {
-            m[k] = __ballot_sync(0xffffffffu, stays[k]);
-            wsum += __popc(m[k]);
-        }
-        if (lane == 0)
-            s_warp[warp] = wsum;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t tot = 0;
-            for (int q = 0; q < kWarps; q++) {
-                const uint32_t c = s_warp[q];
-                s_warp[q] = tot;
-                tot += c;
-            }
-            s_base = tot ? atomicAdd(&ctl->roots[r + 1], tot) : 0u;
-        }
-        __syncthreads();
-        uint32_t pos = s_base + s_warp[warp];
-#pragma unroll
-        for (int k = 0; k < kVItems; k++) {
-            if (stays[k])
-                next[pos + __popc(m[k] & ((1u << lane) - 1))] = x[k];
-            pos += __popc(m[k]);
-        }
-        __syncthreads();  // s_warp / s_base reused next iteration
     }
     // the last block to finish decides the next round (no separate launch)
     __syncthreads();
@@ -845,6 +936,7 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.status = p.status;
     a.forest = reinterpret_cast<unsigned long long *>(p.forest);
     a.ctl = ctx->ctl;
+    a.light_k = p.m;
     return a;
 }
 
@@ -897,7 +989,7 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
         PHEM_TRY(setup_kernels<KIND>(ctx));
         ctx->kernels_ready |= 1u << KIND;
     }
-    const RoundArgs a = make_args(ctx, plan);
+    RoundArgs a = make_args(ctx, plan);
     // light/heavy split: about light_per_vertex * n light edges, and only when
     // the input is at least filter_min_ratio times that large
     // the canonical forest's light edges are the first ones by index, which
@@ -905,6 +997,7 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
     const double lpv = KIND == kKindPacked ? ctx->tune_canonical_light : ctx->tune_light_per_vertex;
     const uint64_t k = (uint64_t)(lpv * (double)plan.n);
     const bool filter = lpv > 0 && k > 0 && (double)plan.m >= ctx->tune_filter_min_ratio * (double)k;
+    a.light_k = filter ? k : plan.m;
     unsigned long long thr = kKeyNone;
     if (filter && KIND == kKindPacked)
         thr = k;  // canonical forest: the first k edges by index are light
@@ -945,13 +1038,10 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
 
 }  // namespace
 
-// Records a survivor list may need: every edge (each flush reserves exactly
-// the records it writes, so a list has no padding).
-uint64_t wl_capacity(uint64_t m, int sm_count)
-{
-    (void)sm_count;
-    return m + 32;
-}
+// Records a survivor list may need: every edge, plus dead padding of at most
+// one list chunk (2048 records) per edge-pass CTA (at most kEpMaxCtasPerSm
+// per SM).
+uint64_t wl_capacity(uint64_t m, int sm_count) { return m + (uint64_t)sm_count * kEpMaxCtasPerSm * 2048; }
 
 // Workspace of one solve: parent (4n), best (8n), two candidate lists (4n
 // each), the MSF bitmap (m / 8) and two survivor lists (16 bytes per record
