@@ -235,6 +235,7 @@ struct MsfPlan {
     unsigned long long *best;// n
     uint32_t *cand[2];       // n each
     uint32_t *bitmap;        // ceil(m / 32)
+    uint32_t *chunk_cnt;     // MSF edges per 1024 edge ids, then their offsets (gather)
     uint4 *wl[2];            // m each
     uint64_t *status;        // look-back status (context-owned), >= tiles
     uint64_t epoch_base;

@@ -58,12 +58,18 @@ struct RoundArgs {
     unsigned long long *best;  // per component: minimum key (w << 32 | id) offered this round
     uint32_t *cand0, *cand1;
     uint32_t *bitmap;
+    uint32_t *chunk_cnt;  // MSF edges per 1024 edge ids (the gather's offsets)
     uint4 *wl0, *wl1;
     uint64_t *status;
     unsigned long long *forest;
     Ctl *ctl;
     uint64_t light_k;  // light edges the threshold aims at (sizes the edge pass's list chunks)
 };
+
+// Count words for the chunks of 1024 edge ids (32 bitmap words) of an m-edge
+// solve: one more so a zero-edge solve still has one, padded to a multiple of
+// 4096 for the scan's vector loads.
+__host__ __device__ inline uint64_t gather_chunks(uint64_t m) { return ((m + 1023) / 1024 + 1 + 4095) / 4096 * 4096; }
 
 // An input record takes part in the forest: self-loops never do; packed CC
 // edges follow union_find_gpu_COO and only count when u < v
@@ -105,9 +111,12 @@ __device__ __forceinline__ void offer_one(unsigned long long *best, OfferCache &
     uint32_t tag = *(volatile uint32_t *)&oc.tag[slot];
     if (tag == kNoTag)
         tag = atomicCAS(&oc.tag[slot], kNoTag, t);
-    if (tag == kNoTag || tag == t)
-        atomicMin(&oc.key[slot], k);
-    else
+    if (tag == kNoTag || tag == t) {
+        // most offers to a hub's slot cannot win: a shared read first avoids
+        // the 64-bit shared atomic (a compare-and-swap loop under contention)
+        if (k < *(volatile unsigned long long *)&oc.key[slot])
+            atomicMin(&oc.key[slot], k);
+    } else
         atomicMin(best + t, k);  // fire and forget: no guard read on the warp's path
 }
 
@@ -393,8 +402,7 @@ __device__ __forceinline__ bool ep_wait(unsigned long long *bar, uint32_t parity
 // fully compressed, so one hop reaches the root).
 template <int KIND, bool LIGHT>
 __device__ __forceinline__ void ep_input_tile(const RoundArgs &a, const unsigned char *stage, bool bulk,
-                                              uint64_t tbase, uint32_t rem, uint32_t thr_hi, uint32_t thr_lo,
-                                              EpWarp &w, uint32_t &filled, uint32_t &flushed, uint4 *out,
+                                              uint64_t tbase, uint32_t rem, unsigned long long thr, EpWarp &w, uint32_t &filled, uint32_t &flushed, uint4 *out,
                                               unsigned long long *len, EpChunks &ch, OfferCache &oc,
                                               uint32_t lane, bool &any_bad)
 {
@@ -433,9 +441,7 @@ __device__ __forceinline__ void ep_input_tile(const RoundArgs &a, const unsigned
         const bool live = inb && e0_live<KIND>(x, y);
         const bool bad = live && max(x, y) >= a.n;
         any_bad |= bad;
-        // e0_key(w, id) < threshold, compared as (high word, low word)
-        const bool light = KIND == kKindMsf ? (z < thr_hi || (z == thr_hi && id < thr_lo))
-                                            : (thr_hi != 0 || id < thr_lo);
+        const bool light = e0_key<KIND>(z, id) < thr;
         keep[j] = live && !bad && (LIGHT ? light : !light);
         u[j] = x;
         v[j] = y;
@@ -522,16 +528,15 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
     const uint64_t full_tiles = count / tile_recs;  // the partial last tile is read directly
     const uint64_t gw = (uint64_t)blockIdx.x * kEpWarps + warp, GW = (uint64_t)gridDim.x * kEpWarps;
     const unsigned long long thr = *(volatile unsigned long long *)&ctl->threshold;
-    const uint32_t thr_hi = (uint32_t)(thr >> 32), thr_lo = (uint32_t)thr;
     const uint64_t policy = l2_evict_first();  // inputs and lists are read once per pass
     if (threadIdx.x == 0) {
-        // chunks of about 1/16 of a CTA's expected survivors (a power of two
-        // in [64, 2048]): few global atomics, and on average half a chunk of
-        // padding per CTA.  Expected: the light edges in round 0, an eighth of
-        // the input in the heavy pass, the whole list in list rounds.
+        // chunks of about a quarter of a CTA's expected survivors (a power of
+        // two in [128, 2048]): few global atomics, and on average half a chunk
+        // of padding per CTA.  Expected: the light edges in round 0, an eighth
+        // of the input in the heavy pass, the whole list in list rounds.
         const uint64_t expect = src == kSrcLight ? a.light_k : (src == kSrcHeavy ? a.m / 8 : count);
-        const uint64_t per = expect / ((uint64_t)gridDim.x * 16);
-        uint32_t c = 64;
+        const uint64_t per = expect / ((uint64_t)gridDim.x * 4);
+        uint32_t c = 128;
         while (c < 2048 && (uint64_t)c * 2 <= per)
             c *= 2;
         s_chunks.size = c;
@@ -587,10 +592,10 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
             ep_list_tile<KIND>(a, in, w.stage[s], bulk, tbase, rem, w, filled, flushed, out, len, s_chunks,
                                s_offers, lane);
         else if (src == kSrcLight)
-            ep_input_tile<KIND, true>(a, w.stage[s], bulk, tbase, rem, thr_hi, thr_lo, w, filled, flushed, out,
+            ep_input_tile<KIND, true>(a, w.stage[s], bulk, tbase, rem, thr, w, filled, flushed, out,
                                       len, s_chunks, s_offers, lane, any_bad);
         else
-            ep_input_tile<KIND, false>(a, w.stage[s], bulk, tbase, rem, thr_hi, thr_lo, w, filled, flushed, out,
+            ep_input_tile<KIND, false>(a, w.stage[s], bulk, tbase, rem, thr, w, filled, flushed, out,
                                        len, s_chunks, s_offers, lane, any_bad);
         fence_proxy_async_smem();  // this lane's reads of the stage precede its refill
         __syncwarp();
@@ -680,6 +685,7 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
             const uint32_t id = rec[q].w;
             a.parent[hk] = tgt;
             atomicOr(a.bitmap + (id >> 5), 1u << (id & 31));
+            atomicAdd(a.chunk_cnt + (id >> 10), 1u);
             if (KIND == kKindPacked && a.forest)
                 a.forest[hk] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
         }
@@ -813,110 +819,122 @@ __device__ void advance_round(Ctl *ctl)
 
 
 // Ordered gather: MSF records ascending by id from the bitmap, plus count and
-// uint64 total weight.
-constexpr uint32_t kGatherIds = 4096;  // ids a tile stages in shared memory (denser tiles use the direct path)
+// uint64 total weight, without a block waiting for another.  The hook counts
+// the edges it marks per chunk of 1024 edge ids (32 bitmap words); one block
+// scans the chunk counts into offsets; then every warp takes whole chunks,
+// ranks its 32 words' bits with a warp scan and gathers its records (12-byte
+// random reads of the input) to out[offset + rank].
+constexpr int kGatherWarps = kWarps;
+
+__global__ void __launch_bounds__(1024) gather_scan_kernel(uint32_t *cnt, uint64_t chunks, Ctl *ctl)
+{
+    // Thread t owns `per` consecutive counts (a multiple of 4, read as
+    // uint4, all loads in flight together); a block scan of the thread sums
+    // gives each run's offset; a second pass writes the exclusive prefixes in
+    // place.  The count array is padded to a multiple of 4 * 1024 words.
+    __shared__ uint32_t s_warp[33];
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint64_t per = (chunks + 4095) / 4096 * 4;
+    uint4 *c4 = reinterpret_cast<uint4 *>(cnt + (uint64_t)threadIdx.x * per);
+    uint32_t sum = 0;
+#pragma unroll 8
+    for (uint64_t q = 0; q < per / 4; q++) {
+        const uint4 v = c4[q];
+        sum += v.x + v.y + v.z + v.w;
+    }
+    uint32_t x = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (uint32_t)d)
+            x += y;
+    }
+    if (lane == 31)
+        s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t v = s_warp[lane];
+        uint32_t vi = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, vi, d);
+            if (lane >= (uint32_t)d)
+                vi += y;
+        }
+        s_warp[lane] = vi - v;
+        if (lane == 31)
+            s_warp[32] = vi;
+    }
+    __syncthreads();
+    uint32_t run = s_warp[warp] + x - sum;
+#pragma unroll 8
+    for (uint64_t q = 0; q < per / 4; q++) {
+        uint4 v = c4[q];
+        const uint4 o = make_uint4(run, run + v.x, run + v.x + v.y, run + v.x + v.y + v.z);
+        run += v.x + v.y + v.z + v.w;
+        c4[q] = o;
+    }
+    if (threadIdx.x == 0)
+        ctl->msf_count = s_warp[32];
+}
 
 __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *out)
 {
-    __shared__ uint32_t s_ids[kGatherIds];
-    __shared__ uint32_t s_tile, s_base;
-    __shared__ uint32_t s_warp[kWarps + 1];
     __shared__ unsigned long long s_red[kWarps];
-    Ctl *ctl = a.ctl;
     const uint64_t words = (a.m + 31) / 32;
-    const uint32_t ntiles = (uint32_t)((words + kTile - 1) / kTile);
-    const uint32_t epoch = a.epoch_base + PHEM_MAX_ROUNDS + 2;
+    const uint64_t chunks = (words + 31) / 32;
+    const uint32_t lane = lane_id();
+    const uint64_t gw = (uint64_t)blockIdx.x * kGatherWarps + (threadIdx.x >> 5);
+    const uint64_t GW = (uint64_t)gridDim.x * kGatherWarps;
     const uint32_t *E = reinterpret_cast<const uint32_t *>(a.e0);
-    for (;;) {
-        if (threadIdx.x == 0)
-            s_tile = atomicAdd(&ctl->out_ticket, 1u);
-        __syncthreads();
-        const uint32_t t = s_tile;
-        if (t >= ntiles)
-            break;
-        const uint64_t wbase = (uint64_t)t * kTile + (uint64_t)threadIdx.x * kItems;
-        uint32_t bits[4];
-        uint32_t c = 0;
+    unsigned long long wsum = 0;
+    for (uint64_t c = gw; c < chunks; c += GW) {
+        const uint64_t wd = c * 32 + lane;
+        uint32_t bits = wd < words ? __ldcs(a.bitmap + wd) : 0u;
+        const uint32_t k = __popc(bits);
+        uint32_t incl = k;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            bits[j] = (wbase + j < words) ? a.bitmap[wbase + j] : 0u;
-            c += __popc(bits[j]);
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (uint32_t)d)
+                incl += y;
         }
-        uint32_t total;
-        const uint32_t off = block_exclusive_scan(c, &total, s_warp);
-        if (threadIdx.x < 32) {
-            const uint32_t ex = lookback_exclusive(a.status, t, total, epoch, &ctl->err);
-            if (threadIdx.x == 0) {
-                s_base = ex;
-                if (t == ntiles - 1)
-                    ctl->msf_count = (unsigned long long)ex + total;
-            }
-        }
-        unsigned long long wsum = 0;
-        if (total <= kGatherIds) {
-            // the tile's ids go to shared memory in order, then every thread
-            // gathers independent records (coalesced writes, loads in flight)
-            uint32_t pos = off;
+        uint64_t pos = (uint64_t)__ldcs(a.chunk_cnt + c) + (incl - k);
+        // four of the lane's records per step, their loads in flight together
+        while (bits) {
+            uint32_t id[4];
+            int cntq = 0;
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                uint32_t b = bits[j];
-                while (b) {
-                    const int k = __ffs(b) - 1;
-                    b &= b - 1;
-                    s_ids[pos++] = (uint32_t)((wbase + j) * 32 + k);
+            for (int q = 0; q < 4; q++) {
+                id[q] = 0xffffffffu;
+                if (bits) {
+                    id[q] = (uint32_t)(wd * 32 + (__ffs(bits) - 1));
+                    bits &= bits - 1;
+                    cntq++;
                 }
             }
-            __syncthreads();
-            const uint32_t base = s_base;
-            for (uint32_t i0 = 0; i0 < total; i0 += kBlock * 4) {
-                phem_edge e[4];
+            phem_edge e[4];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const uint32_t i = i0 + q * kBlock + threadIdx.x;
-                    e[q] = phem_edge{0, 0, 0};
-                    if (i < total) {
-                        const uint64_t id = s_ids[i];
-                        e[q].u = __ldg(E + id * 3);
-                        e[q].v = __ldg(E + id * 3 + 1);
-                        e[q].w = __ldg(E + id * 3 + 2);
-                    }
+            for (int q = 0; q < 4; q++)
+                if (id[q] != 0xffffffffu) {
+                    const uint64_t i3 = (uint64_t)id[q] * 3;
+                    e[q].u = __ldg(E + i3);
+                    e[q].v = __ldg(E + i3 + 1);
+                    e[q].w = __ldg(E + i3 + 2);
                 }
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const uint32_t i = i0 + q * kBlock + threadIdx.x;
-                    if (i < total) {
-                        if (out)
-                            out[base + i] = e[q];
-                        wsum += e[q].w;
-                    }
-                }
-            }
-        } else {
-            __syncthreads();
-            uint32_t pos = s_base + off;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                uint32_t b = bits[j];
-                while (b) {
-                    const int k = __ffs(b) - 1;
-                    b &= b - 1;
-                    const uint64_t id = (wbase + j) * 32 + k;
-                    phem_edge e;
-                    e.u = __ldg(E + id * 3);
-                    e.v = __ldg(E + id * 3 + 1);
-                    e.w = __ldg(E + id * 3 + 2);
+            for (int q = 0; q < 4; q++)
+                if (q < cntq) {
                     if (out)
-                        out[pos] = e;
+                        out[pos] = e[q];
                     pos++;
-                    wsum += e.w;
+                    wsum += e[q].w;
                 }
-            }
         }
-        const unsigned long long bs = block_sum_u64(wsum, s_red);
-        if (threadIdx.x == 0 && bs)
-            atomicAdd(&ctl->msf_total, bs);
-        __syncthreads();
     }
+    const unsigned long long bs = block_sum_u64(wsum, s_red);
+    if (threadIdx.x == 0 && bs)
+        atomicAdd(&a.ctl->msf_total, bs);
 }
 
 RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
@@ -931,6 +949,7 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.cand0 = p.cand[0];
     a.cand1 = p.cand[1];
     a.bitmap = p.bitmap;
+    a.chunk_cnt = p.chunk_cnt;
     a.wl0 = p.wl[0];
     a.wl1 = p.wl[1];
     a.status = p.status;
@@ -1003,6 +1022,7 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
         thr = k;  // canonical forest: the first k edges by index are light
     PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), s));
     PHEM_CUDA_TRY(cudaMemsetAsync(plan.bitmap, 0, ((plan.m + 31) / 32) * sizeof(uint32_t), s));
+    PHEM_CUDA_TRY(cudaMemsetAsync(plan.chunk_cnt, 0, gather_chunks(plan.m) * sizeof(uint32_t), s));
     {
         KernelScope ks(ctx, kKInit);
         init_kernel<<<vertex_blocks(ctx, plan.n), kBlock, 0, s>>>(a, thr);
@@ -1055,6 +1075,7 @@ size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
     c.take<uint32_t>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>((m + 31) / 32 + 4);
+    c.take<uint32_t>(gather_chunks(m));
     c.take<uint4>(wl_capacity(m, sm_count));
     c.take<uint4>(wl_capacity(m, sm_count));
     return c.off;
@@ -1068,7 +1089,6 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     c.off = core;
     const size_t extra_at = c.take<uint8_t>(extra_bytes);
     PHEM_TRY(ws_reserve(ctx, c.off));
-    PHEM_TRY(status_reserve(ctx, (m + kTile - 1) / kTile + 2));
     char *base = static_cast<char *>(ctx->ws);
     Carve k;
     plan->status = ctx->status;
@@ -1077,6 +1097,7 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     plan->cand[0] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
+    plan->chunk_cnt = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(gather_chunks(m)));
     plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->wl[1] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->e0 = d_e0;
@@ -1100,11 +1121,17 @@ phem_status msf_run(phem_context *ctx, int kind, MsfPlan &plan, uint32_t *rounds
 phem_status msf_gather(phem_context *ctx, MsfPlan &plan, phem_edge *d_out)
 {
     const RoundArgs a = make_args(ctx, plan);
-    const uint64_t words = (plan.m + 31) / 32;
-    const uint64_t tiles = (words + kTile - 1) / kTile;
-    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->gather_blocks));
-    KernelScope k(ctx, kKGather);
-    gather_kernel<<<blocks, kBlock, 0, ctx->stream>>>(a, d_out);
+    const uint64_t chunks = gather_chunks(plan.m);
+    {
+        KernelScope k(ctx, kKGather);
+        gather_scan_kernel<<<1, 1024, 0, ctx->stream>>>(plan.chunk_cnt, chunks, ctx->ctl);
+    }
+    const uint64_t blocks_needed = (chunks + kGatherWarps - 1) / kGatherWarps;
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks_needed, (uint64_t)ctx->gather_blocks));
+    {
+        KernelScope k(ctx, kKGather);
+        gather_kernel<<<blocks, kBlock, 0, ctx->stream>>>(a, d_out);
+    }
     PHEM_CUDA_TRY(cudaGetLastError());
     return PHEM_OK;
 }
