@@ -88,14 +88,19 @@ __device__ __forceinline__ unsigned long long e0_key(uint32_t w, uint64_t id)
     return KIND == kKindMsf ? (((unsigned long long)w << 32) | id) : (unsigned long long)id;
 }
 
-// Per-CTA pre-reduction of offers.  Most survivors of hub-heavy rounds (and
-// the heavy pass, whose records mostly touch the light phase's giant
-// component) offer to a handful of roots, and atomics on one best[] word
-// serialise on its L2 slice.  A root claims the slot hash(t) of a 512-entry
-// table in shared memory on its first offer; offers to a claimed slot are
-// shared-memory atomicMins, offers that collide with another root go to
-// best[] directly, and the table is flushed to best[] (one atomic per slot)
-// when the CTA's pass ends.  Shared: tags 2 KB, keys 4 KB.
+// Offers.  A survivor offers its key to both of its roots' best[] words.
+// Most survivors of hub-heavy rounds (and of the heavy pass, whose records
+// mostly touch the light phase's giant component) offer to a handful of
+// roots, and atomics on one best[] word serialise on its L2 slice; so a root
+// first tries the slot hash(t) of a 512-entry table in the CTA's shared
+// memory, claiming it when it is free: offers to a claimed slot are
+// shared-memory atomicMins behind a shared read, and the table goes to best[]
+// (one atomic per slot) when the CTA's pass ends.  An offer whose slot another
+// root holds reads best[t] from L2 first and issues the 64-bit atomicMin only
+// when it can still win: the read may be stale but never below the true
+// value.  Both roots' reads are issued before either atomic.  (Grouping a
+// warp's equal targets with __match_any_sync and reduce first cost more than
+// the atomics it saved.)  Shared: tags 2 KB, keys 4 KB.
 constexpr int kOfferSlots = 512;
 constexpr uint32_t kNoTag = 0xffffffffu;
 
@@ -104,44 +109,33 @@ struct OfferCache {
     uint32_t tag[kOfferSlots];
 };
 
-__device__ __forceinline__ void offer_one(unsigned long long *best, OfferCache &oc, uint32_t t,
-                                          unsigned long long k)
+// True when the offer went to (or lost against) t's shared slot.
+__device__ __forceinline__ bool table_offer(OfferCache &oc, uint32_t t, unsigned long long k)
 {
     const int slot = (int)((t * 0x9E3779B1u) >> 23);  // 9 bits
     uint32_t tag = *(volatile uint32_t *)&oc.tag[slot];
     if (tag == kNoTag)
         tag = atomicCAS(&oc.tag[slot], kNoTag, t);
-    if (tag == kNoTag || tag == t) {
-        // most offers to a hub's slot cannot win: a shared read first avoids
-        // the 64-bit shared atomic (a compare-and-swap loop under contention)
-        if (k < *(volatile unsigned long long *)&oc.key[slot])
-            atomicMin(&oc.key[slot], k);
-    } else
-        atomicMin(best + t, k);  // fire and forget: no guard read on the warp's path
+    if (tag != kNoTag && tag != t)
+        return false;
+    // most offers to a hub's slot cannot win: a shared read first avoids the
+    // 64-bit shared atomic (a compare-and-swap loop under contention)
+    if (k < *(volatile unsigned long long *)&oc.key[slot])
+        atomicMin(&oc.key[slot], k);
+    return true;
 }
 
-// Offers `key` to best[ta] and best[tb] for the live lanes of a warp.  Lanes
-// with the same target are grouped (__match_any_sync) and their keys reduced
-// (high word, then low word among the lanes holding the minimum high word)
-// so each group makes one offer: a hub's records arrive in runs.  Every lane
-// of the warp calls this, converged.
 __device__ __forceinline__ void offer_pair(unsigned long long *best, OfferCache &oc, uint32_t ta, uint32_t tb,
                                            unsigned long long key, bool on)
 {
-    const unsigned act = __ballot_sync(0xffffffffu, on);
     if (!on)
         return;
-    const uint32_t hi = (uint32_t)(key >> 32), lo = (uint32_t)key;
-    const unsigned pa = __match_any_sync(act, ta);
-    const unsigned pb = __match_any_sync(act, tb);
-    const uint32_t ahi = __reduce_min_sync(pa, hi), bhi = __reduce_min_sync(pb, hi);
-    const uint32_t alo = __reduce_min_sync(pa, hi == ahi ? lo : 0xffffffffu);
-    const uint32_t blo = __reduce_min_sync(pb, hi == bhi ? lo : 0xffffffffu);
-    const uint32_t lane = lane_id();
-    if ((int)lane == __ffs(pa) - 1)
-        offer_one(best, oc, ta, ((unsigned long long)ahi << 32) | alo);
-    if ((int)lane == __ffs(pb) - 1)
-        offer_one(best, oc, tb, ((unsigned long long)bhi << 32) | blo);
+    const bool da = table_offer(oc, ta, key), db = table_offer(oc, tb, key);
+    const unsigned long long ga = da ? 0ull : __ldcg(best + ta), gb = db ? 0ull : __ldcg(best + tb);
+    if (!da && key < ga)
+        atomicMin(best + ta, key);
+    if (!db && key < gb)
+        atomicMin(best + tb, key);
 }
 
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
@@ -636,17 +630,36 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
 // (new_grafting_edges, MST/src/kernels.cu:73-134).  Dead padding records
 // (equal roots) are skipped.  The list was just written, so it is mostly read
 // from L2.
+// Chooser ids staged per warp before they go to the chooser list: a warp
+// flushes once more than 256 are pending (an iteration adds at most 256),
+// with one atomicAdd per flush and no barrier between warps.
+constexpr uint32_t kHookBuf = 512;
+
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
 {
-    __shared__ uint32_t s_warp[kWarps + 1];
-    __shared__ unsigned long long s_base;
+    __shared__ uint32_t s_buf[kWarps][kHookBuf];
     Ctl *ctl = a.ctl;
     if (!*(volatile uint32_t *)&ctl->go)
         return;
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const uint64_t len = ctl->wl_len[r];
     const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    uint32_t *buf = s_buf[warp];
+    uint32_t pend = 0;  // warp-uniform
+    auto flush = [&]() {
+        __syncwarp();
+        unsigned long long base = 0;
+        if (lane == 0)
+            base = atomicAdd(&ctl->n_r[r], (unsigned long long)pend);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        for (uint32_t i = lane; i < pend; i += 32)
+            a.cand0[base + i] = buf[i];
+        __syncwarp();
+        pend = 0;
+    };
     const uint64_t step = (uint64_t)gridDim.x * kBlock * 4;
     for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * 4; i0 < len; i0 += step) {
         uint4 rec[4];
@@ -661,53 +674,47 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
             ka[q] = real ? __ldg(a.best + rec[q].x) : 0ull;
             kb[q] = real ? __ldg(a.best + rec[q].y) : 0ull;
         }
-        uint32_t choosers = 0;  // bit 2q: rec q chosen by its first root, 2q + 1: by its second
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            if (rec[q].x == rec[q].y)
-                continue;
             const unsigned long long key = ((unsigned long long)rec[q].z << 32) | rec[q].w;
-            const bool A = ka[q] == key, B = kb[q] == key;
-            if (!A && !B)
-                continue;
-            choosers |= ((uint32_t)A << (2 * q)) | ((uint32_t)B << (2 * q + 1));
-            uint32_t hk, tgt;
-            if (A && B) {
-                hk = rec[q].x > rec[q].y ? rec[q].x : rec[q].y;
-                tgt = rec[q].x > rec[q].y ? rec[q].y : rec[q].x;
-            } else if (A) {
-                hk = rec[q].x;
-                tgt = rec[q].y;
-            } else {
-                hk = rec[q].y;
-                tgt = rec[q].x;
+            const bool real = rec[q].x != rec[q].y;
+            const bool A = real && ka[q] == key, B = real && kb[q] == key;
+            if (A || B) {
+                uint32_t hk, tgt;
+                if (A && B) {
+                    hk = rec[q].x > rec[q].y ? rec[q].x : rec[q].y;
+                    tgt = rec[q].x > rec[q].y ? rec[q].y : rec[q].x;
+                } else if (A) {
+                    hk = rec[q].x;
+                    tgt = rec[q].y;
+                } else {
+                    hk = rec[q].y;
+                    tgt = rec[q].x;
+                }
+                const uint32_t id = rec[q].w;
+                a.parent[hk] = tgt;
+                atomicOr(a.bitmap + (id >> 5), 1u << (id & 31));
+                atomicAdd(a.chunk_cnt + (id >> 10), 1u);
+                if (KIND == kKindPacked && a.forest)
+                    a.forest[hk] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
             }
-            const uint32_t id = rec[q].w;
-            a.parent[hk] = tgt;
-            atomicOr(a.bitmap + (id >> 5), 1u << (id & 31));
-            atomicAdd(a.chunk_cnt + (id >> 10), 1u);
-            if (KIND == kKindPacked && a.forest)
-                a.forest[hk] = __ldg(reinterpret_cast<const unsigned long long *>(a.e0) + id);
+            // the round's choosers (each component finds its one record) go
+            // to the chooser list, which the compress walks instead of all
+            // vertices
+            const unsigned ma = __ballot_sync(0xffffffffu, A);
+            if (A)
+                buf[pend + __popc(ma & below)] = rec[q].x;
+            pend += __popc(ma);
+            const unsigned mb = __ballot_sync(0xffffffffu, B);
+            if (B)
+                buf[pend + __popc(mb & below)] = rec[q].y;
+            pend += __popc(mb);
         }
-        // the round's choosers (each component finds its one record) go to
-        // the chooser list, which the compress walks instead of all vertices
-        uint32_t total;
-        uint32_t off = block_exclusive_scan(__popc(choosers), &total, s_warp);
-        if (total == 0)
-            continue;  // uniform
-        if (threadIdx.x == 0)
-            s_base = atomicAdd(&ctl->n_r[r], (unsigned long long)total);
-        __syncthreads();
-        const unsigned long long base = s_base;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (choosers & (1u << (2 * q)))
-                a.cand0[base + off++] = rec[q].x;
-            if (choosers & (1u << (2 * q + 1)))
-                a.cand0[base + off++] = rec[q].y;
-        }
-        __syncthreads();  // s_warp and s_base are reused
+        if (pend > kHookBuf - 256)
+            flush();
     }
+    if (pend)
+        flush();
 }
 
 constexpr int kVItems = 4;  // candidates per thread per iteration of the vertex kernels
