@@ -449,9 +449,10 @@ def _served_stream(torch, srv, pool, rates, requests: int, rng, h2d_gbs: float) 
         idx = rng.integers(0, len(pool), requests)
         reqs = [pool[i] for i in idx]
         arr = poisson_arrivals(requests, rate, seed=rate)
-        t0 = time.perf_counter()
         res = srv.replay(reqs, arr)
-        wall = time.perf_counter() - t0
+        # the served span on the server's own clock: first submission to last
+        # result (building the requests in Python is not serving time)
+        wall = (max(r.done_ns for r in res) - min(r.submit_ns for r in res)) / 1e9
         assert all(r.status == 0 for r in res)
         lat = np.array([r.latency_ns for r in res]) / 1e6
         e = sum(g.m for g in reqs)
@@ -850,18 +851,43 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
-def profile_traffic(name: str):
-    """Per-launch DRAM traffic of a kernel from its committed ncu summary, if any."""
-    p = ROOT / "profiles" / f"{name}.md"
+_UNITS = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}
+
+
+def profile_traffic(kernel: str, csv_name: str, solves: int):
+    """DRAM bytes (read + write) per solve of every launch of `kernel`, from the
+    ncu CSV that the capture command in profiles/ wrote (--csv --log-file):
+    the capture profiles `solves` solves; None when the file is absent."""
+    import csv
+    p = ROOT / "profiles" / csv_name
     if not p.exists():
         return None
-    for ln in p.read_text().splitlines():
-        if ln.startswith("traffic_bytes_per_solve:"):
-            try:
-                return float(ln.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+    lines = [ln for ln in p.read_text().splitlines() if ln.startswith('"')]
+    total = 0.0
+    for row in csv.DictReader(lines):
+        if kernel in row.get("Kernel Name", "") and row.get("Metric Name") in ("dram__bytes_read.sum",
+                                                                                "dram__bytes_write.sum"):
+            total += float(row["Metric Value"].replace(",", "")) * _UNITS.get(row.get("Metric Unit", "byte"), 1)
+    return total / solves if total else None
+
+
+def profile_solves(args) -> None:
+    """--profile-solves N: N plain solves of the benchmark workload on device
+    memory and nothing else, a fixed target for per-launch profiles."""
+    import torch
+
+    import phem_graph_b200 as P
+    g, E = rmat22(0, args.scale, args.edge_factor)
+    ctx = P.Context(0)
+    d = torch.from_numpy(E.view(np.int32)).to("cuda:0")
+    o = torch.empty((g.n, 3), dtype=torch.int32, device="cuda:0")
+    ct = torch.zeros(2, dtype=torch.int64, device="cuda:0")
+    for _ in range(args.profile_solves):
+        r = ctx.msf_solve_device(d, g.m, g.n, o, ct)
+    torch.cuda.synchronize()
+    print(json.dumps({"solves": args.profile_solves, "m": g.m, "n": g.n, "count": r.count, "total": r.total,
+                      "rounds": r.rounds}))
+    ctx.close()
 
 
 def main() -> None:
@@ -882,6 +908,8 @@ def main() -> None:
                          "host memory (scale 28: 4.29 G edges, beyond one solve's 2^32 limit)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the connected-components, batched and served workloads")
+    ap.add_argument("--profile-solves", type=int, default=0, metavar="N",
+                    help="N plain solves of the workload on device memory (a fixed profiler target), then exit")
     ap.add_argument("--profile-sample", action="store_true",
                     help="one small call of every kernel family (a fixed target for profilers), then exit")
     ap.add_argument("--ingest-only", type=int, default=0, metavar="SCALE",
@@ -894,6 +922,9 @@ def main() -> None:
         return
     if args.profile_sample:
         profile_sample()
+        return
+    if args.profile_solves:
+        profile_solves(args)
         return
     if args.impl == "reference":
         run_reference(args)
@@ -972,6 +1003,14 @@ def main() -> None:
             r_host = ctx.msf_solve(h_edges, n, out=h_res)
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t0) / e2e_steps
+        # the host link alone: one plain pinned copy of the same edges
+        d_copy = torch.empty_like(h_pinned, device=f"cuda:{local}")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d_copy.copy_(h_pinned, non_blocking=True)
+        torch.cuda.synchronize()
+        copy_s = time.perf_counter() - t0
+        del d_copy
     if world > 1:
         tt = torch.tensor([t_ms, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -1006,10 +1045,13 @@ def main() -> None:
     roofline = None
     if dom:
         achieved = kernels[dom].get("achieved_gbs")
-        traffic = profile_traffic(f"{dom}_rmat22")
+        traffic = (profile_traffic("edge_pass", "msf_edge_pass_rmat22_dram.csv", 2)
+                   if (dom == "msf_edge_pass" and args.scale == 22 and args.edge_factor == 16) else None)
         roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
-                    "traffic": traffic, "traffic_basis": "DRAM bytes per solve (all launches), profiles/",
+                    "traffic": traffic,
+                    "traffic_basis": "ncu dram__bytes_read + write of the edge-pass launches of one solve "
+                                     "(profiles/msf_edge_pass_rmat22_dram.csv, bench.py --profile-solves 2)",
                     "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)",
                     "algorithmic_bytes_per_step": byts.get(dom)}
     solve_gbs = byts["survey"] / (ms_per_step / 1e3) / 1e9 if byts["survey"] else None
@@ -1032,7 +1074,9 @@ def main() -> None:
         "result": {"msf_edges": stats.count, "total_weight": stats.total, "rounds": stats.rounds},
         "e2e": {"value": world * m / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": m * 12,
                 "d2h_bytes_per_step": r_host.count * 12 + 16, "ms_per_step": e2e_s * 1e3,
-                "api": "phem_msf_solve (C ABI), pinned host edges"},
+                "plain_copy_ms": copy_s * 1e3,
+                "api": "phem_msf_solve (C ABI), pinned host edges (four chunks, each solved while the next "
+                       "is copied)"},
         "gpu_launches": gpu_launches,
         "clocks": clocks.summary(),
     }

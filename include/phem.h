@@ -113,10 +113,14 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *   "msf.light_per_vertex"  light edges per vertex taken by the MSF filter
  *                           before the heavy pass; 0 disables the filter   [0.5]
  *   "msf.filter_min_ratio"  filter only when m >= ratio * light edges      [2.0]
- *   "msf.first_batch"       Boruvka rounds queued before the first check  [8]
+ *   "msf.first_batch"       Boruvka rounds queued before the first check  [12]
  *   "msf.next_batch"        rounds queued per later check                 [4]
  *   "msf.edge_ctas_per_sm"  CTAs of 8 independent warps per SM in the edge
  *                           pass, 1 to 4                                  [4]
+ *   "msf.graph"             1: the Boruvka rounds run as a cached CUDA graph
+ *                           whose while-node the device drives; 0: rounds
+ *                           queued on the stream in batches (per-launch
+ *                           profiling always uses the stream form)        [1]
  *   "cc.canonical_light_per_vertex"  msf.light_per_vertex for the
  *                           PHEM_CC_CANONICAL forest (light = first by index) [2]
  *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
@@ -256,7 +260,11 @@ phem_status phem_cc_solve_noalloc(const uint64_t *d_edges, int64_t m, int32_t n,
  *                     n - 1 records and may be NULL;
  *   *count, *total <- number of MSF edges and their uint64 total weight.
  * Self-loops are ignored.  Endpoints must be < n.  m < 2^32.  count, total and
- * stats may be NULL. */
+ * stats may be NULL.  Host edges of 2^24 or more are solved as phem_msf_stream
+ * solves them, in four chunks copied while the chunk before is solved (the
+ * forest is the same, record for record); stats then holds the last chunk's
+ * per-round counts, the whole forest's count and total, and device_ms from
+ * the first copy to the last solve. */
 phem_status phem_msf_solve(phem_context *ctx, const phem_edge *edges, uint64_t m, uint32_t n,
                            phem_edge *msf, uint64_t *count, uint64_t *total, phem_msf_stats *stats);
 

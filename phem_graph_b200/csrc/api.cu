@@ -306,6 +306,9 @@ void phem_context_destroy(phem_context *ctx)
     DeviceGuard g(ctx->device);
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    for (auto &e : ctx->msf_exec)
+        if (e)
+            cudaGraphExecDestroy(e);
     if (ctx->ws)
         cudaFree(ctx->ws);
     if (ctx->input)
@@ -428,6 +431,8 @@ phem_status phem_context_set_tuning(phem_context *ctx, const char *key, double v
         ctx->tune_first_batch = (int)value;
     } else if (k == "msf.next_batch" && value >= 1 && value <= PHEM_MAX_ROUNDS) {
         ctx->tune_next_batch = (int)value;
+    } else if (k == "msf.graph" && (value == 0 || value == 1)) {
+        ctx->tune_graph = (int)value;
     } else if (k == "msf.edge_ctas_per_sm" && value >= 1 && value <= 4 && value == (int)value) {
         ctx->tune_edge_ctas = (int)value;
         ctx->kernels_ready = 0;  // the grid size is recomputed at the next solve
@@ -466,6 +471,8 @@ phem_status phem_context_get_tuning(phem_context *ctx, const char *key, double *
         *value = ctx->tune_first_batch;
     else if (k == "msf.next_batch")
         *value = ctx->tune_next_batch;
+    else if (k == "msf.graph")
+        *value = ctx->tune_graph;
     else if (k == "msf.edge_ctas_per_sm")
         *value = ctx->tune_edge_ctas;
     else if (k == "cc.sample_per_vertex")
@@ -822,11 +829,29 @@ static phem_status msf_common(phem_context *ctx, const phem_edge *edges, uint64_
     return PHEM_OK;
 }
 
+static phem_status msf_stream_impl(phem_context *ctx, const phem_edge *h_edges, uint64_t m, uint32_t n,
+                                   uint64_t chunk, phem_edge *msf, uint64_t *count, uint64_t *total, float *ms,
+                                   phem_msf_stats *last_stats);
+
+// Host MSF inputs of this many edges or more are solved in four chunks while
+// the next chunk is copied (see phem_msf_solve).
+constexpr uint64_t kMsfOverlapMinEdges = 1ull << 24;
+
 phem_status phem_msf_solve(phem_context *ctx, const phem_edge *edges, uint64_t m, uint32_t n, phem_edge *msf,
                            uint64_t *count, uint64_t *total, phem_msf_stats *stats)
 {
     PHEM_TRY(check_ctx(ctx));
     DeviceGuard g(ctx->device);
+    // A large host input would otherwise be copied whole before the solve
+    // starts.  Solved in four chunks instead -- chunk k with the forest of the
+    // chunks before it while chunk k + 1 is copied -- the copy hides every
+    // solve but the last, and the forest is the same (the chunked solve is
+    // exact, record for record).
+    const uint64_t chunk = ((m + 3) / 4 + 3) & ~3ull;
+    const uint64_t R = ((uint64_t)n + 2) & ~3ull;
+    if (m >= kMsfOverlapMinEdges && edges && !is_device_ptr(edges) && n > 1 && n < UINT32_MAX && R < kMaxEdges &&
+        chunk <= kMaxEdges - R && R < chunk)
+        return msf_stream_impl(ctx, edges, m, n, chunk, msf, count, total, nullptr, stats);
     return msf_common(ctx, edges, m, n, msf, count, total, stats, nullptr);
 }
 
@@ -857,6 +882,15 @@ phem_status phem_msf_solve_device(phem_context *ctx, const phem_edge *d_edges, u
 // stream while chunk k is solved.
 phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_t m, uint32_t n, uint64_t chunk,
                             phem_edge *msf, uint64_t *count, uint64_t *total, float *ms)
+{
+    return msf_stream_impl(ctx, h_edges, m, n, chunk, msf, count, total, ms, nullptr);
+}
+
+// last_stats (may be NULL): the per-round counts of the last chunk's solve,
+// with the whole forest's count and total.
+static phem_status msf_stream_impl(phem_context *ctx, const phem_edge *h_edges, uint64_t m, uint32_t n,
+                                   uint64_t chunk, phem_edge *msf, uint64_t *count, uint64_t *total, float *ms,
+                                   phem_msf_stats *last_stats)
 {
     PHEM_TRY(check_ctx(ctx));
     const uint64_t R = ((uint64_t)n + 2) & ~3ull;  // n - 1 rounded up to a multiple of 4
@@ -937,7 +971,8 @@ phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_
             st = PHEM_ERR_CUDA;
             break;
         }
-        st = msf_common(ctx, cur + start, R - start + len, n, d_out, &carried, &weight, nullptr, nullptr);
+        st = msf_common(ctx, cur + start, R - start + len, n, d_out, &carried, &weight,
+                        k + 1 == chunks ? last_stats : nullptr, nullptr);
         // the forest goes directly before the next chunk
         if (st == PHEM_OK && k + 1 < chunks && carried &&
             cudaMemcpyAsync(slot[(k + 1) & 1] + R - carried, d_out, carried * sizeof(phem_edge),
@@ -971,6 +1006,11 @@ phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_
         *total = weight;
     if (ms)
         *ms = t;
+    if (last_stats) {
+        last_stats->device_ms = t;  // first copy to last solve
+        last_stats->msf_edges = carried;
+        last_stats->total_weight = weight;
+    }
     return PHEM_OK;
 }
 

@@ -47,11 +47,15 @@ struct phem_context {
     uint32_t kernels_ready = 0;        // bit k: launch attributes of edge kind k are set
     int gather_blocks = 0;
     int tune_edge_ctas = 4;              // MSF edge pass: CTAs (of 8 independent warps) per SM, 1 to 4
+    int tune_graph = 1;                  // MSF rounds as a CUDA graph with a device-driven while-node
+    cudaGraphExec_t msf_exec[2] = {nullptr, nullptr};  // cached round-loop graphs, per edge kind
+    uint64_t msf_key[2][40] = {};        // what each was built for
+    uint64_t msf_seen[2][40] = {};       // the last solve's key (a graph is built when it repeats)
     // tuning knobs (phem_context_set_tuning)
     double tune_light_per_vertex = 0.5;  // light edges per vertex in the MSF filter (0: no filter)
     double tune_canonical_light = 2.0;   // the same for the canonical CC forest (edges by index)
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
-    int tune_first_batch = 8;            // Boruvka rounds queued before the first host check
+    int tune_first_batch = 12;           // Boruvka rounds queued before the first host check
     int tune_next_batch = 4;             // rounds queued per later check
     int tune_batch_block = 1024;         // batched kernel: threads per CTA
     int tune_batch_items = 4;            // batched kernel: records per thread per step

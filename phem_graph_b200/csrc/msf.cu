@@ -53,7 +53,6 @@ struct RoundArgs {
     const void *e0;
     uint64_t m;
     uint32_t n;
-    uint32_t epoch_base;
     uint32_t *parent;
     unsigned long long *best;  // per component: minimum key (w << 32 | id) offered this round
     uint32_t *cand0, *cand1;
@@ -196,11 +195,19 @@ __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const 
     __shared__ uint32_t hist[2048];
     __shared__ uint32_t s_prefix, s_rank;
     const int tid = threadIdx.x;
-    for (int i = tid; i < kSample; i += kSelectThreads) {
+    // all of a thread's sample loads in flight together
+    constexpr int kPerThread = kSample / kSelectThreads;
+    uint32_t v[kPerThread];
+#pragma unroll
+    for (int q = 0; q < kPerThread; q++) {
+        const int i = tid + q * kSelectThreads;
         const uint64_t lo = (uint64_t)i * m / kSample, hi = (uint64_t)(i + 1) * m / kSample;
         const uint64_t pos = hi > lo ? lo + mix64(0x5EED0000ull + i) % (hi - lo) : lo;
-        samp[i] = e0[pos * 3 + 2];
+        v[q] = __ldg(e0 + pos * 3 + 2);
     }
+#pragma unroll
+    for (int q = 0; q < kPerThread; q++)
+        samp[tid + q * kSelectThreads] = v[q];
     if (tid == 0) {
         s_prefix = 0;
         s_rank = (uint32_t)(k * kSample / m);
@@ -313,9 +320,9 @@ __device__ __forceinline__ void ring_append(EpWarp &w, uint32_t &filled, bool ke
 // CTA's last chunk is padded with dead records {0, 0, 0, 0} (equal roots:
 // the next pass drops them) when the pass ends.
 struct EpChunks {
-    unsigned long long state;    // (chunk number << 32) | slots handed out in it
-    unsigned long long base[8];  // list index of chunk c at [c & 7]
+    uint32_t state;              // (chunk number mod 256) << 24 | slots handed out in it
     uint32_t size;               // records per chunk
+    unsigned long long base[8];  // list index of chunk c at [c & 7]
 };
 
 // Slots of one request: [b1, b1 + split) then [b2, b2 + k - split).
@@ -330,26 +337,29 @@ __device__ __noinline__ EpSlots chunk_reserve(EpChunks &c, unsigned long long *l
 {
     const uint32_t C = c.size;
     for (uint32_t spins = 0; spins < kMbarSpinCap; spins++) {
-        const unsigned long long old = atomicAdd(&c.state, (unsigned long long)k);
-        __threadfence_block();
-        const uint32_t cid = (uint32_t)(old >> 32), used = (uint32_t)old;
+        // no fence on this path: the base read depends on the chunk number
+        // the atomic returned, and the closer publishes the base before it
+        // publishes that number
+        const uint32_t old = atomicAdd(&c.state, k);
+        const uint32_t cid = old >> 24, used = old & 0xffffffu;
         if (used + k <= C) {
             const unsigned long long b = *(volatile unsigned long long *)&c.base[cid & 7] + used;
             return EpSlots{b, b, k};
         }
         if (used <= C) {
             // this request closes chunk cid (its last C - used slots; none for
-            // the empty chunk 0) and opens chunk cid + 1 with the rest
-            const uint32_t split = cid > 0 ? C - used : 0;
-            const unsigned long long b1 = cid > 0 ? *(volatile unsigned long long *)&c.base[cid & 7] + used : 0;
+            // the empty chunk 0 of the pass) and opens chunk cid + 1 with the rest
+            const uint32_t split = used < C ? C - used : 0;
+            const unsigned long long b1 = split ? *(volatile unsigned long long *)&c.base[cid & 7] + used : 0;
             const unsigned long long nb = atomicAdd(len, (unsigned long long)C);
-            *(volatile unsigned long long *)&c.base[(cid + 1) & 7] = nb;
+            const uint32_t next = (cid + 1) & 0xffu;
+            *(volatile unsigned long long *)&c.base[next & 7] = nb;
             __threadfence_block();
-            atomicExch(&c.state, ((unsigned long long)(cid + 1) << 32) | (k - split));
+            atomicExch(&c.state, (next << 24) | (k - split));
             return EpSlots{b1, nb, split};
         }
         // another warp is opening the next chunk
-        while ((uint32_t)(*(volatile unsigned long long *)&c.state >> 32) == cid)
+        while ((*(volatile uint32_t *)&c.state >> 24) == cid)
             if (++spins >= kMbarSpinCap)
                 break;
     }
@@ -534,7 +544,7 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
         while (c < 2048 && (uint64_t)c * 2 <= per)
             c *= 2;
         s_chunks.size = c;
-        s_chunks.state = (unsigned long long)c;  // chunk 0 "full": the first request opens chunk 1
+        s_chunks.state = c;  // chunk 0 "full" (and empty): the first request opens chunk 1
     }
     for (int i = threadIdx.x; i < kOfferSlots; i += kEpThreads) {
         s_offers.tag[i] = kNoTag;
@@ -615,9 +625,9 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
         if (t != kNoTag)
             atomicMin(a.best + t, s_offers.key[i]);
     }
-    const unsigned long long st = s_chunks.state;
-    const uint32_t cid = (uint32_t)(st >> 32), used = min((uint32_t)st, s_chunks.size);
-    if (cid > 0)
+    const uint32_t st = s_chunks.state;
+    const uint32_t cid = st >> 24, used = min(st & 0xffffffu, s_chunks.size);
+    if (s_chunks.state != s_chunks.size)  // a chunk was opened
         for (uint32_t i = used + threadIdx.x; i < s_chunks.size; i += kEpThreads)
             out[s_chunks.base[cid & 7] + i] = make_uint4(0, 0, 0, 0);
 }
@@ -726,11 +736,18 @@ constexpr int kVItems = 4;  // candidates per thread per iteration of the vertex
 // hop.
 __device__ void advance_round(Ctl *ctl);
 
-__global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
+// `loop`: when the rounds run as a CUDA graph's while-node, the handle of its
+// condition, which the block that decides the next round sets to the continue
+// flag (use_loop 0: rounds queued on a stream).
+__global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a, cudaGraphConditionalHandle loop,
+                                                          int use_loop)
 {
     Ctl *ctl = a.ctl;
-    if (!*(volatile uint32_t *)&ctl->go)
+    if (!*(volatile uint32_t *)&ctl->go) {
+        if (use_loop && blockIdx.x == 0 && threadIdx.x == 0)
+            cudaGraphSetConditional(loop, 0);
         return;
+    }
     const uint32_t r = *(volatile uint32_t *)&ctl->round;
     const bool full = *(volatile uint32_t *)&ctl->phase == 0 && ctl->m_r[r] == 0;
     const uint64_t count = full ? a.n : ctl->n_r[r];
@@ -788,6 +805,8 @@ __global__ void __launch_bounds__(kBlock) compress_kernel(RoundArgs a)
             __threadfence();
             ctl->misc[6] = 0;
             advance_round(ctl);
+            if (use_loop)
+                cudaGraphSetConditional(loop, ctl->go);
         }
     }
 }
@@ -947,10 +966,10 @@ __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *
 RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
 {
     RoundArgs a;
+    std::memset(&a, 0, sizeof(a));  // no stray padding bytes: the graph cache compares args bytewise
     a.e0 = p.e0;
     a.m = p.m;
     a.n = p.n;
-    a.epoch_base = (uint32_t)p.epoch_base;
     a.parent = p.parent;
     a.best = p.best;
     a.cand0 = p.cand[0];
@@ -989,7 +1008,7 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
         KernelScope k(ctx, kKCompress);
         // four CTAs per SM: enough walks in flight for the all-vertex rounds,
         // and a short launch for the late rounds' few candidates
-        compress_kernel<<<std::min(vb, ctx->sm_count * 4), kBlock, 0, ctx->stream>>>(a);
+        compress_kernel<<<std::min(vb, ctx->sm_count * 4), kBlock, 0, ctx->stream>>>(a, 0, 0);
     }
     PHEM_CUDA_TRY(cudaGetLastError());
     return PHEM_OK;
@@ -1004,6 +1023,117 @@ phem_status setup_kernels(phem_context *ctx)
     ctx->edge_pass_blocks = ctx->sm_count * std::max(1, std::min(per_sm, want));
     PHEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, kBlock, 0));
     ctx->gather_blocks = ctx->sm_count * std::max(1, per_sm);
+    return PHEM_OK;
+}
+
+// The round loop as a CUDA graph: memsets, init, threshold select, then a
+// while-node whose body is one round (edge pass, hook, compress) and whose
+// condition the compress's deciding block sets to the continue flag.  The
+// device runs exactly the rounds the solve needs, with no host round trip and
+// no round queued after convergence.  The executable graph is cached in the
+// context and rebuilt when anything baked into its nodes changes (buffers,
+// sizes, grids, threshold).
+struct GraphKey {
+    RoundArgs a;
+    unsigned long long thr;
+    uint64_t k;
+    int select, ep_blocks, vb_init, vb_comp, hook_blocks, kind;
+};
+
+template <class... Args>
+phem_status add_kernel(cudaGraphNode_t *node, cudaGraph_t g, const cudaGraphNode_t *dep, void (*fn)(Args...),
+                       dim3 grid, dim3 block, void **args)
+{
+    cudaKernelNodeParams p{};
+    p.func = reinterpret_cast<void *>(fn);
+    p.gridDim = grid;
+    p.blockDim = block;
+    p.sharedMemBytes = 0;
+    p.kernelParams = args;
+    PHEM_CUDA_TRY(cudaGraphAddKernelNode(node, g, dep, dep ? 1 : 0, &p));
+    return PHEM_OK;
+}
+
+phem_status add_memset(cudaGraphNode_t *node, cudaGraph_t g, const cudaGraphNode_t *dep, void *dst, size_t bytes)
+{
+    cudaMemsetParams p{};
+    p.dst = dst;
+    p.value = 0;
+    p.elementSize = 1;
+    p.width = bytes;
+    p.height = 1;
+    p.pitch = bytes;
+    PHEM_CUDA_TRY(cudaGraphAddMemsetNode(node, g, dep, dep ? 1 : 0, &p));
+    return PHEM_OK;
+}
+
+template <int KIND>
+phem_status build_graph(phem_context *ctx, const MsfPlan &plan, const GraphKey &key, cudaGraphExec_t *exec)
+{
+    cudaGraph_t g = nullptr;
+    PHEM_CUDA_TRY(cudaGraphCreate(&g, 0));
+    struct Drop {
+        cudaGraph_t g;
+        ~Drop() { cudaGraphDestroy(g); }
+    } drop{g};
+    cudaGraphNode_t last, nn;
+    RoundArgs a = key.a;
+    unsigned long long thr = key.thr;
+    PHEM_TRY(add_memset(&last, g, nullptr, ctx->ctl, sizeof(Ctl)));
+    const size_t bitmap_bytes = ((plan.m + 31) / 32) * sizeof(uint32_t);
+    if (bitmap_bytes) {  // a memset node of zero bytes is invalid
+        PHEM_TRY(add_memset(&nn, g, &last, plan.bitmap, bitmap_bytes));
+        last = nn;
+    }
+    PHEM_TRY(add_memset(&nn, g, &last, plan.chunk_cnt, gather_chunks(plan.m) * sizeof(uint32_t)));
+    last = nn;
+    {
+        void *args[] = {&a, &thr};
+        PHEM_TRY(add_kernel(&nn, g, &last, init_kernel, dim3(key.vb_init), dim3(kBlock), args));
+    }
+    last = nn;
+    const uint32_t *e0w = static_cast<const uint32_t *>(plan.e0);
+    uint64_t m = plan.m, k = key.k;
+    Ctl *ctl = ctx->ctl;
+    if (key.select) {
+        void *args[] = {&e0w, &m, &k, &ctl};
+        cudaGraphNode_t ns;
+        PHEM_TRY(add_kernel(&ns, g, &last, select_threshold_kernel, dim3(1), dim3(kSelectThreads), args));
+        last = ns;
+    }
+    cudaGraphConditionalHandle loop;
+    PHEM_CUDA_TRY(cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t nc;
+    PHEM_CUDA_TRY(cudaGraphAddNode(&nc, g, &last, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaGraphNode_t b0, b1, b2;
+    {
+        void *args[] = {&a};
+        PHEM_TRY(add_kernel(&b0, body, nullptr, edge_pass_kernel<KIND>, dim3(key.ep_blocks), dim3(kEpThreads), args));
+        PHEM_TRY(add_kernel(&b1, body, &b0, hook_kernel<KIND>, dim3(key.hook_blocks), dim3(kBlock), args));
+    }
+    {
+        int use = 1;
+        void *args[] = {&a, &loop, &use};
+        PHEM_TRY(add_kernel(&b2, body, &b1, compress_kernel, dim3(key.vb_comp), dim3(kBlock), args));
+    }
+    if (*exec) {
+        // same topology (the cached graph had a select node iff this one has):
+        // update the instantiated graph's parameters in place, which costs
+        // far less than instantiating again
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(*exec, g, &info) == cudaSuccess)
+            return PHEM_OK;
+        cudaGetLastError();
+        cudaGraphExecDestroy(*exec);
+        *exec = nullptr;
+    }
+    PHEM_CUDA_TRY(cudaGraphInstantiate(exec, g, 0));
     return PHEM_OK;
 }
 
@@ -1027,6 +1157,56 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
     unsigned long long thr = kKeyNone;
     if (filter && KIND == kKindPacked)
         thr = k;  // canonical forest: the first k edges by index are light
+    if (!ctx->profiling && ctx->tune_graph) {
+        // the graph form (per-launch event timing needs the stream form)
+        GraphKey key;
+        std::memset(&key, 0, sizeof(key));
+        key.a = a;
+        key.thr = thr;
+        key.k = k;
+        key.select = filter && KIND == kKindMsf;
+        key.ep_blocks = ctx->edge_pass_blocks;
+        key.vb_init = vertex_blocks(ctx, plan.n);
+        key.vb_comp = std::min(vertex_blocks(ctx, plan.n), ctx->sm_count * 4);
+        key.hook_blocks = ctx->sm_count * 4;
+        key.kind = KIND;
+        const bool cached = ctx->msf_exec[KIND] && std::memcmp(ctx->msf_key[KIND], &key, sizeof(key)) == 0;
+        // a graph is built only for a solve seen twice in a row (same
+        // buffers, sizes and grids): one-off shapes take the stream form
+        // instead of paying for a graph they would use once
+        const bool repeat = std::memcmp(ctx->msf_seen[KIND], &key, sizeof(key)) == 0;
+        std::memcpy(ctx->msf_seen[KIND], &key, sizeof(key));
+        if (!cached && !repeat)
+            goto stream_form;
+        if (!cached) {
+            GraphKey old;
+            std::memcpy(&old, ctx->msf_key[KIND], sizeof(old));
+            if (ctx->msf_exec[KIND] && old.select != key.select) {
+                cudaGraphExecDestroy(ctx->msf_exec[KIND]);
+                ctx->msf_exec[KIND] = nullptr;
+            }
+            std::memset(ctx->msf_key[KIND], 0, sizeof(ctx->msf_key[KIND]));
+            PHEM_TRY(build_graph<KIND>(ctx, plan, key, &ctx->msf_exec[KIND]));
+            static_assert(sizeof(GraphKey) <= sizeof(ctx->msf_key[0]), "graph key storage");
+            std::memcpy(ctx->msf_key[KIND], &key, sizeof(key));
+        }
+        PHEM_CUDA_TRY(cudaGraphLaunch(ctx->msf_exec[KIND], s));
+        PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+        PHEM_TRY(stream_wait(ctx));
+        const Ctl &h = *ctx->h_ctl;
+        // launches the graph made: init, select, three per round
+        ctx->launches[kKInit] += 1;
+        ctx->launches[kKSelect] += key.select ? 1 : 0;
+        ctx->launches[kKEdgePass] += h.round;
+        ctx->launches[kKHook] += h.round;
+        ctx->launches[kKCompress] += h.round;
+        if (h.go)
+            return ctl_status(h.err | kErrRounds, "msf");
+        if (rounds_out)
+            *rounds_out = h.round;
+        return ctl_status(h.err, "msf");
+    }
+stream_form:
     PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), s));
     PHEM_CUDA_TRY(cudaMemsetAsync(plan.bitmap, 0, ((plan.m + 31) / 32) * sizeof(uint32_t), s));
     PHEM_CUDA_TRY(cudaMemsetAsync(plan.chunk_cnt, 0, gather_chunks(plan.m) * sizeof(uint32_t), s));

@@ -38,6 +38,8 @@ class Served:
     queue_ns: int
     forest: np.ndarray | None   # MSF: (count, 3) uint32 ascending by edge id
     labels: np.ndarray | None   # CC: min-id labels
+    submit_ns: int = 0          # steady-clock times of submission and completion (native)
+    done_ns: int = 0
 
 
 class Server:
@@ -93,7 +95,8 @@ class Server:
             else:
                 labels = out
         return Served(int(res.status), int(res.path), int(res.forest_edges), int(res.total_weight),
-                      int(res.done_ns - res.submit_ns), int(res.start_ns - res.submit_ns), forest, labels)
+                      int(res.done_ns - res.submit_ns), int(res.start_ns - res.submit_ns), forest, labels,
+                      int(res.submit_ns), int(res.done_ns))
 
     def solve(self, g: ServedGraph) -> Served:
         """Submits one request and waits for it."""

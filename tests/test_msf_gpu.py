@@ -278,3 +278,29 @@ def test_edge_pass_grid_sizes(ctx, ctas):
     assert_msf(r, E, ids, cnt, tot)
     np.testing.assert_array_equal(rc.labels, labels)
     np.testing.assert_array_equal(P.api.forest_set(rc.forest), oracle.forest_set(forest))
+
+
+@pytest.mark.parametrize("graph", [0, 1])
+def test_graph_and_stream_round_loops(ctx, graph):
+    """The rounds as a CUDA graph with a device-driven while-node and as
+    batches queued on the stream give the same forest and round counts, for
+    weighted and packed (canonical CC) edges, across calls whose sizes differ
+    (the cached graph is updated or rebuilt)."""
+    old = ctx.get_tuning("msf.graph")
+    ctx.set_tuning("msf.graph", graph)
+    try:
+        for scale, seed in ((12, 31), (14, 32), (12, 31)):
+            g = gen.rmat_graph(scale, 8, seed=seed)
+            E = g.msf_edges()
+            ids, cnt, tot = expect(E, g.n)
+            r = ctx.msf_solve(E, g.n)
+            assert_msf(r, E, ids, cnt, tot)
+            _, _, _, m_r, n_r = oracle.msf_boruvka(E, g.n)
+            assert r.rounds >= 1
+        c = gen.er_graph(1 << 14, 1 << 16, seed=33)
+        labels, forest = oracle.cc_solve(c.pairs, c.n)
+        rc = ctx.cc_solve(c.pairs, c.n, canonical=True)
+        np.testing.assert_array_equal(rc.labels, labels)
+        np.testing.assert_array_equal(P.api.forest_set(rc.forest), oracle.forest_set(forest))
+    finally:
+        ctx.set_tuning("msf.graph", old)
