@@ -474,7 +474,7 @@ def _served_stream(torch, srv, pool, rates, requests: int, rng, h2d_gbs: float) 
             "pool_graphs": len(pool), "pool_edges": pool_edges}
 
 
-def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), requests: int = 2000) -> dict:
+def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), requests: int = 2000, slots: int = 2) -> dict:
     """Served request streams (Poisson arrivals at each offered rate, 2000
     requests per rate, a 64 GB device budget, request buffers in pinned host
     memory):
@@ -503,9 +503,9 @@ def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), requests: int 
     h2d_gbs = 8 * (1 << 25) / (time.perf_counter() - t0) / 1e9
     del h, d
     rng = np.random.default_rng(1)
-    cfg = {"memory_budget_gb": 64, "slots": 2, "max_batch_graphs": 1024, "large_edges": 1 << 18,
+    cfg = {"memory_budget_gb": 64, "slots": slots, "max_batch_graphs": 1024, "large_edges": 1 << 18,
            "large_workers": 2, "requests_per_rate": requests, "h2d_gbs": h2d_gbs}
-    with Server(memory_budget=64 << 30, slots=2, max_batch_graphs=1024, large_edges=1 << 18,
+    with Server(memory_budget=64 << 30, slots=slots, max_batch_graphs=1024, large_edges=1 << 18,
                 large_workers=2) as srv:
         out_mixed = _served_stream(torch, srv, mixed, rates, requests, rng, h2d_gbs)
         out_small = _served_stream(torch, srv, small, rates, requests, rng, h2d_gbs)

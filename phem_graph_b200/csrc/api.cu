@@ -793,14 +793,18 @@ static phem_status msf_common(phem_context *ctx, const phem_edge *edges, uint64_
     plan.e0 = se.dev;
     Timed timer(ctx);
     uint32_t rounds = 0;
-    PHEM_TRY(msf_run(ctx, kKindMsf, plan, &rounds));
+    // rounds, gather and the count copy are queued back to back; one wait at
+    // the end (a host round trip between them would leave the GPU idle)
+    PHEM_TRY(msf_run(ctx, kKindMsf, plan, &rounds, true));
     PHEM_TRY(msf_gather(ctx, plan, static_cast<phem_edge *>(so.dev)));
-    const float ms = timer.stop();
+    PHEM_CUDA_TRY(cudaEventRecord(ctx->ev_stop, ctx->stream));
     if (d_count_total)
         PHEM_CUDA_TRY(cudaMemcpyAsync(d_count_total, &ctx->ctl->msf_count, 2 * sizeof(uint64_t),
                                       cudaMemcpyDeviceToDevice, ctx->stream));
-    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
-    PHEM_TRY(stream_wait(ctx));
+    PHEM_TRY(msf_finish(ctx, &rounds));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) != cudaSuccess)
+        ms = 0.f;
     const Ctl &h = *ctx->h_ctl;
     PHEM_TRY(ctl_status(h.err, "msf"));
     if (h.msf_count > (uint64_t)n - 1 + (n == 0)) {

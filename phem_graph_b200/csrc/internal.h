@@ -51,6 +51,8 @@ struct phem_context {
     cudaGraphExec_t msf_exec[2] = {nullptr, nullptr};  // cached round-loop graphs, per edge kind
     uint64_t msf_key[2][40] = {};        // what each was built for
     uint64_t msf_seen[2][40] = {};       // the last solve's key (a graph is built when it repeats)
+    bool msf_graph_pending = false;      // a graph solve's launches are still to be counted
+    bool msf_graph_select = false;       // ... and it had a threshold select
     // tuning knobs (phem_context_set_tuning)
     double tune_light_per_vertex = 0.5;  // light edges per vertex in the MSF filter (0: no filter)
     double tune_canonical_light = 2.0;   // the same for the canonical CC forest (edges by index)
@@ -249,9 +251,15 @@ struct MsfPlan {
 size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count);
 phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, uint32_t n, size_t extra_bytes,
                      MsfPlan *plan, size_t *extra_off);
-// Queues the whole Boruvka solve; returns after the rounds are done (host
-// checks the round flag between rounds).  On return the bitmap marks the MSF.
-phem_status msf_run(phem_context *ctx, int kind, MsfPlan &plan, uint32_t *rounds_out);
+// Queues the whole Boruvka solve; returns after the rounds are done and
+// checked (the stream form checks the round flag between batches).  With
+// `deferred` the graph form returns once the rounds are queued, and the
+// caller queues more work before msf_finish waits and checks.  After the
+// rounds the bitmap marks the MSF.
+phem_status msf_run(phem_context *ctx, int kind, MsfPlan &plan, uint32_t *rounds_out, bool deferred = false);
+// Waits for the queued work and checks the rounds (copies the control block
+// to ctx->h_ctl).
+phem_status msf_finish(phem_context *ctx, uint32_t *rounds_out);
 // Queues the ordered gather of MSF edges (kKindMsf): out[0..count) + count/total into ctl.
 phem_status msf_gather(phem_context *ctx, MsfPlan &plan, phem_edge *d_out);
 

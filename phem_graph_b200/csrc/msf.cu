@@ -1138,7 +1138,7 @@ phem_status build_graph(phem_context *ctx, const MsfPlan &plan, const GraphKey &
 }
 
 template <int KIND>
-phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
+phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out, bool deferred)
 {
     cudaStream_t s = ctx->stream;
     if (!(ctx->kernels_ready & (1u << KIND))) {
@@ -1191,20 +1191,11 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out)
             std::memcpy(ctx->msf_key[KIND], &key, sizeof(key));
         }
         PHEM_CUDA_TRY(cudaGraphLaunch(ctx->msf_exec[KIND], s));
-        PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
-        PHEM_TRY(stream_wait(ctx));
-        const Ctl &h = *ctx->h_ctl;
-        // launches the graph made: init, select, three per round
-        ctx->launches[kKInit] += 1;
-        ctx->launches[kKSelect] += key.select ? 1 : 0;
-        ctx->launches[kKEdgePass] += h.round;
-        ctx->launches[kKHook] += h.round;
-        ctx->launches[kKCompress] += h.round;
-        if (h.go)
-            return ctl_status(h.err | kErrRounds, "msf");
-        if (rounds_out)
-            *rounds_out = h.round;
-        return ctl_status(h.err, "msf");
+        ctx->msf_graph_select = key.select;
+        ctx->msf_graph_pending = true;
+        if (deferred)
+            return PHEM_OK;  // msf_finish waits and checks, after the caller queued more work
+        return msf_finish(ctx, rounds_out);
     }
 stream_form:
     PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), s));
@@ -1233,17 +1224,34 @@ stream_form:
             break;
         batch = ctx->tune_next_batch;
     }
-    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    ctx->msf_graph_pending = false;
+    if (deferred)
+        return PHEM_OK;
+    return msf_finish(ctx, rounds_out);
+}
+
+}  // namespace
+
+phem_status msf_finish(phem_context *ctx, uint32_t *rounds_out)
+{
+    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
     PHEM_TRY(stream_wait(ctx));
     const Ctl &h = *ctx->h_ctl;
+    if (ctx->msf_graph_pending) {
+        // launches the graph made: init, select, three per round
+        ctx->launches[kKInit] += 1;
+        ctx->launches[kKSelect] += ctx->msf_graph_select ? 1 : 0;
+        ctx->launches[kKEdgePass] += h.round;
+        ctx->launches[kKHook] += h.round;
+        ctx->launches[kKCompress] += h.round;
+        ctx->msf_graph_pending = false;
+    }
     if (h.go)
         return ctl_status(h.err | kErrRounds, "msf");
     if (rounds_out)
         *rounds_out = h.round;
     return ctl_status(h.err, "msf");
 }
-
-}  // namespace
 
 // Records a survivor list may need: every edge, plus dead padding of at most
 // one list chunk (2048 records) per edge-pass CTA (at most kEpMaxCtasPerSm
@@ -1298,11 +1306,11 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     return PHEM_OK;
 }
 
-phem_status msf_run(phem_context *ctx, int kind, MsfPlan &plan, uint32_t *rounds_out)
+phem_status msf_run(phem_context *ctx, int kind, MsfPlan &plan, uint32_t *rounds_out, bool deferred)
 {
     if (kind == kKindMsf)
-        return run_impl<kKindMsf>(ctx, plan, rounds_out);
-    return run_impl<kKindPacked>(ctx, plan, rounds_out);
+        return run_impl<kKindMsf>(ctx, plan, rounds_out, deferred);
+    return run_impl<kKindPacked>(ctx, plan, rounds_out, deferred);
 }
 
 phem_status msf_gather(phem_context *ctx, MsfPlan &plan, phem_edge *d_out)

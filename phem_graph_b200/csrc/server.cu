@@ -151,7 +151,7 @@ struct phem_server {
     // or its labels) is host work proportional to the result, so the requests
     // of a large batch are split over a few threads: on one thread it capped
     // the batched path at about 40 k small requests per second.
-    static constexpr size_t kRetireThreads = 4;
+    static constexpr size_t kRetireThreads = 8;
     static constexpr size_t kRetireSerialBelow = 64;  // requests; fewer are finished on this thread
 
     void retire_range(Slot &s, phem_status st, bool cuda_ok, size_t lo, size_t hi)
