@@ -474,7 +474,7 @@ def _served_stream(torch, srv, pool, rates, requests: int, rng, h2d_gbs: float) 
             "pool_graphs": len(pool), "pool_edges": pool_edges}
 
 
-def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), requests: int = 2000, slots: int = 2) -> dict:
+def bench_served(torch, rates=(1000, 3000, 10000, 30000, 100000), requests: int = 2000, slots: int = 4) -> dict:
     """Served request streams (Poisson arrivals at each offered rate, 2000
     requests per rate, a 64 GB device budget, request buffers in pinned host
     memory):
