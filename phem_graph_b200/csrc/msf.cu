@@ -70,6 +70,11 @@ struct RoundArgs {
 // 4096 for the scan's vector loads.
 __host__ __device__ inline uint64_t gather_chunks(uint64_t m) { return ((m + 1023) / 1024 + 1 + 4095) / 4096 * 4096; }
 
+// Survivor records mark in the top bit of each root whether the record's
+// offer may have won there; vertex ids leave that bit free up to this n.
+constexpr uint32_t kMarkMaxN = 0x80000000u;
+constexpr uint32_t kRootMask = 0x7fffffffu;
+
 // An input record takes part in the forest: self-loops never do; packed CC
 // edges follow union_find_gpu_COO and only count when u < v
 // (CC/ExternalSpanningTree.cu:82).
@@ -108,8 +113,9 @@ struct OfferCache {
     uint32_t tag[kOfferSlots];
 };
 
-// True when the offer went to (or lost against) t's shared slot.
-__device__ __forceinline__ bool table_offer(OfferCache &oc, uint32_t t, unsigned long long k)
+// True when the offer went to (or lost against) t's shared slot; *may is set
+// when it went there below the slot's value.
+__device__ __forceinline__ bool table_offer(OfferCache &oc, uint32_t t, unsigned long long k, int *may)
 {
     const int slot = (int)((t * 0x9E3779B1u) >> 23);  // 9 bits
     uint32_t tag = *(volatile uint32_t *)&oc.tag[slot];
@@ -119,22 +125,34 @@ __device__ __forceinline__ bool table_offer(OfferCache &oc, uint32_t t, unsigned
         return false;
     // most offers to a hub's slot cannot win: a shared read first avoids the
     // 64-bit shared atomic (a compare-and-swap loop under contention)
-    if (k < *(volatile unsigned long long *)&oc.key[slot])
+    if (k < *(volatile unsigned long long *)&oc.key[slot]) {
         atomicMin(&oc.key[slot], k);
+        *may = 1;
+    }
     return true;
 }
 
-__device__ __forceinline__ void offer_pair(unsigned long long *best, OfferCache &oc, uint32_t ta, uint32_t tb,
-                                           unsigned long long key, bool on)
+// Returns bit 0 / bit 1 set when the offer at ta / tb may still win.  A
+// cleared bit means the key lost there for good: it met a lower value (the
+// shared slot's, or best[t]'s in L2), and the final minimum is lower still
+// (keys are unique).
+__device__ __forceinline__ uint32_t offer_pair(unsigned long long *best, OfferCache &oc, uint32_t ta, uint32_t tb,
+                                               unsigned long long key, bool on)
 {
     if (!on)
-        return;
-    const bool da = table_offer(oc, ta, key), db = table_offer(oc, tb, key);
+        return 0u;
+    int wa = 0, wb = 0;
+    const bool da = table_offer(oc, ta, key, &wa), db = table_offer(oc, tb, key, &wb);
     const unsigned long long ga = da ? 0ull : __ldcg(best + ta), gb = db ? 0ull : __ldcg(best + tb);
-    if (!da && key < ga)
+    if (!da && key < ga) {
         atomicMin(best + ta, key);
-    if (!db && key < gb)
+        wa = 1;
+    }
+    if (!db && key < gb) {
         atomicMin(best + tb, key);
+        wb = 1;
+    }
+    return (uint32_t)wa | ((uint32_t)wb << 1);
 }
 
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long *s)
@@ -331,16 +349,13 @@ struct EpSlots {
     uint32_t split;
 };
 
-// Reserves k (1..32) list slots; split = 0 and b1 = ~0 when a wait for a new
-// chunk gave up (the status bit is set).  Lane 0 only.
-__device__ __noinline__ EpSlots chunk_reserve(EpChunks &c, unsigned long long *len, uint32_t k, uint32_t *err)
+// The rare part of a reservation: `old` is what the first atomicAdd
+// returned and did not fit (close the chunk, or wait for the warp closing it).
+__device__ __noinline__ EpSlots chunk_reserve_slow(EpChunks &c, unsigned long long *len, uint32_t k, uint32_t *err,
+                                                   uint32_t old)
 {
     const uint32_t C = c.size;
     for (uint32_t spins = 0; spins < kMbarSpinCap; spins++) {
-        // no fence on this path: the base read depends on the chunk number
-        // the atomic returned, and the closer publishes the base before it
-        // publishes that number
-        const uint32_t old = atomicAdd(&c.state, k);
         const uint32_t cid = old >> 24, used = old & 0xffffffu;
         if (used + k <= C) {
             const unsigned long long b = *(volatile unsigned long long *)&c.base[cid & 7] + used;
@@ -362,9 +377,25 @@ __device__ __noinline__ EpSlots chunk_reserve(EpChunks &c, unsigned long long *l
         while ((*(volatile uint32_t *)&c.state >> 24) == cid)
             if (++spins >= kMbarSpinCap)
                 break;
+        old = atomicAdd(&c.state, k);
     }
     set_err(err, kErrLookback);
     return EpSlots{~0ull, ~0ull, 0};
+}
+
+// Reserves k (1..32) list slots; b1 = b2 = ~0 when a wait for a new chunk
+// gave up (the status bit is set).  Lane 0 only.  No fence on the common
+// path: the base read depends on the chunk number the atomic returned, and
+// the closer publishes the base before it publishes that number.
+__device__ __forceinline__ EpSlots chunk_reserve(EpChunks &c, unsigned long long *len, uint32_t k, uint32_t *err)
+{
+    const uint32_t old = atomicAdd(&c.state, k);
+    const uint32_t cid = old >> 24, used = old & 0xffffffu;
+    if (used + k <= c.size) {
+        const unsigned long long b = *(volatile unsigned long long *)&c.base[cid & 7] + used;
+        return EpSlots{b, b, k};
+    }
+    return chunk_reserve_slow(c, len, k, err, old);
 }
 
 // Writes the `cnt` (<= 32) oldest ring entries to the list and offers them.
@@ -383,11 +414,18 @@ __device__ __forceinline__ void ring_flush(const RoundArgs &a, uint4 *out, unsig
     const unsigned long long b1 = __shfl_sync(0xffffffffu, sl.b1, 0), b2 = __shfl_sync(0xffffffffu, sl.b2, 0);
     const uint32_t split = __shfl_sync(0xffffffffu, sl.split, 0);
     if (b2 != ~0ull) {
-        if (on)
-            out[lane < split ? b1 + lane : b2 + (lane - split)] = rec;
         const unsigned long long key =
             KIND == kKindMsf ? (((unsigned long long)rec.z << 32) | rec.w) : (unsigned long long)rec.w;
-        offer_pair(a.best, oc, rec.x, rec.y, key, on);
+        const uint32_t may = offer_pair(a.best, oc, rec.x, rec.y, key, on);
+        // the hook only looks at the roots where the record may have won
+        // (the top bit of a root is free when n <= 2^31)
+        uint4 r = rec;
+        if (a.n <= kMarkMaxN) {
+            r.x |= (may & 1u) << 31;
+            r.y |= (may & 2u) << 30;
+        }
+        if (on)
+            out[lane < split ? b1 + lane : b2 + (lane - split)] = r;
     }
     __syncwarp();  // the ring slots just read may be written again
 }
@@ -493,11 +531,12 @@ __device__ __forceinline__ void ep_list_tile(const RoundArgs &a, const uint4 *in
         else if (keep[j])
             rec[j] = __ldcs(in + tbase + idx);
     }
+    const uint32_t rmask = a.n <= kMarkMaxN ? kRootMask : 0xffffffffu;  // drop the last round's marks
 #pragma unroll
     for (int j = 0; j < ROWS; j++)
         if (keep[j]) {
-            rec[j].x = __ldg(a.parent + rec[j].x);
-            rec[j].y = __ldg(a.parent + rec[j].y);
+            rec[j].x = __ldg(a.parent + (rec[j].x & rmask));
+            rec[j].y = __ldg(a.parent + (rec[j].y & rmask));
         }
 #pragma unroll
     for (int j = 0; j < ROWS; j++) {
@@ -657,6 +696,8 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
     const uint4 *wl = (r & 1) ? a.wl1 : a.wl0;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
+    const bool marks = a.n <= kMarkMaxN;
+    const uint32_t rmask = marks ? kRootMask : 0xffffffffu;
     uint32_t *buf = s_buf[warp];
     uint32_t pend = 0;  // warp-uniform
     auto flush = [&]() {
@@ -678,11 +719,16 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
         for (int q = 0; q < 4; q++) {
             const uint64_t i = i0 + q * kBlock + threadIdx.x;
             rec[q] = i < len ? __ldcg(wl + i) : make_uint4(0, 0, 0, 0);
-            const bool real = rec[q].x != rec[q].y;
+            // only the roots where the record's offer may have won (marked by
+            // the edge pass; every root when n is too large for marks)
+            const bool ma = marks ? (rec[q].x >> 31) != 0 : rec[q].x != rec[q].y;
+            const bool mb = marks ? (rec[q].y >> 31) != 0 : rec[q].x != rec[q].y;
+            rec[q].x &= rmask;
+            rec[q].y &= rmask;
             // best is read-only during this kernel: cached loads let the
             // few hub components of late rounds hit in L1
-            ka[q] = real ? __ldg(a.best + rec[q].x) : 0ull;
-            kb[q] = real ? __ldg(a.best + rec[q].y) : 0ull;
+            ka[q] = ma ? __ldg(a.best + rec[q].x) : 0ull;
+            kb[q] = mb ? __ldg(a.best + rec[q].y) : 0ull;
         }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
