@@ -57,7 +57,7 @@ struct RoundArgs {
     unsigned long long *best;  // per component: minimum key (w << 32 | id) offered this round
     uint32_t *cand0, *cand1;
     uint32_t *bitmap;
-    uint32_t *chunk_cnt;  // MSF edges per 1024 edge ids (the gather's offsets)
+    uint32_t *chunk_cnt;  // MSF edges per 1024 edge ids, then per-4096-chunk totals and offsets
     uint4 *wl0, *wl1;
     uint64_t *status;
     unsigned long long *forest;
@@ -69,6 +69,10 @@ struct RoundArgs {
 // solve: one more so a zero-edge solve still has one, padded to a multiple of
 // 4096 for the scan's vector loads.
 __host__ __device__ inline uint64_t gather_chunks(uint64_t m) { return ((m + 1023) / 1024 + 1 + 4095) / 4096 * 4096; }
+// Scan tiles of 4096 counts, and the count array's storage: the counts, then
+// the tiles' totals and their exclusive prefixes.
+__host__ __device__ inline uint64_t gather_tiles(uint64_t m) { return gather_chunks(m) / 4096; }
+__host__ __device__ inline uint64_t gather_words(uint64_t m) { return gather_chunks(m) + 2 * gather_tiles(m) + 4; }
 
 // Survivor records mark in the top bit of each root whether the record's
 // offer may have won there; vertex ids leave that bit free up to this n.
@@ -898,56 +902,74 @@ __device__ void advance_round(Ctl *ctl)
 // random reads of the input) to out[offset + rank].
 constexpr int kGatherWarps = kWarps;
 
-__global__ void __launch_bounds__(1024) gather_scan_kernel(uint32_t *cnt, uint64_t chunks, Ctl *ctl)
+// Offsets of the chunks' records: every block scans one tile of 4096 counts
+// in place (exclusive, within the tile; one uint4 per thread) and publishes
+// the tile's total; the last block to finish scans the totals into the
+// tiles' offsets and the forest size.  No block waits for another.
+__global__ void __launch_bounds__(1024) gather_scan_kernel(uint32_t *cnt, uint64_t tiles, Ctl *ctl)
 {
-    // Thread t owns `per` consecutive counts (a multiple of 4, read as
-    // uint4, all loads in flight together); a block scan of the thread sums
-    // gives each run's offset; a second pass writes the exclusive prefixes in
-    // place.  The count array is padded to a multiple of 4 * 1024 words.
     __shared__ uint32_t s_warp[33];
+    __shared__ bool s_last;
+    uint32_t *tile_total = cnt + tiles * 4096, *tile_off = tile_total + tiles;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    const uint64_t per = (chunks + 4095) / 4096 * 4;
-    uint4 *c4 = reinterpret_cast<uint4 *>(cnt + (uint64_t)threadIdx.x * per);
-    uint32_t sum = 0;
-#pragma unroll 8
-    for (uint64_t q = 0; q < per / 4; q++) {
-        const uint4 v = c4[q];
-        sum += v.x + v.y + v.z + v.w;
-    }
-    uint32_t x = sum;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-        if (lane >= (uint32_t)d)
-            x += y;
-    }
-    if (lane == 31)
-        s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t v = s_warp[lane];
-        uint32_t vi = v;
+    auto block_scan = [&](uint32_t v, uint32_t *total) {  // exclusive scan over the block
+        uint32_t x = v;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, vi, d);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
             if (lane >= (uint32_t)d)
-                vi += y;
+                x += y;
         }
-        s_warp[lane] = vi - v;
         if (lane == 31)
-            s_warp[32] = vi;
+            s_warp[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t w = s_warp[lane];
+            uint32_t wi = w;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, wi, d);
+                if (lane >= (uint32_t)d)
+                    wi += y;
+            }
+            s_warp[lane] = wi - w;
+            if (lane == 31)
+                s_warp[32] = wi;
+        }
+        __syncthreads();
+        *total = s_warp[32];
+        const uint32_t r = s_warp[warp] + x - v;
+        __syncthreads();  // s_warp is reused
+        return r;
+    };
+    uint4 *c4 = reinterpret_cast<uint4 *>(cnt + (uint64_t)blockIdx.x * 4096) + threadIdx.x;
+    const uint4 v = *c4;
+    uint32_t total;
+    const uint32_t run = block_scan(v.x + v.y + v.z + v.w, &total);
+    *c4 = make_uint4(run, run + v.x, run + v.x + v.y, run + v.x + v.y + v.z);
+    if (threadIdx.x == 0) {
+        tile_total[blockIdx.x] = total;
+        __threadfence();
+        s_last = atomicAdd(&ctl->misc[5], 1ull) == gridDim.x - 1;
     }
     __syncthreads();
-    uint32_t run = s_warp[warp] + x - sum;
-#pragma unroll 8
-    for (uint64_t q = 0; q < per / 4; q++) {
-        uint4 v = c4[q];
-        const uint4 o = make_uint4(run, run + v.x, run + v.x + v.y, run + v.x + v.y + v.z);
-        run += v.x + v.y + v.z + v.w;
-        c4[q] = o;
+    if (!s_last)
+        return;
+    __threadfence();
+    if (threadIdx.x == 0)
+        ctl->misc[5] = 0;
+    uint32_t carry = 0;
+    for (uint64_t t0 = 0; t0 < tiles; t0 += 1024) {
+        const uint64_t t = t0 + threadIdx.x;
+        const uint32_t tv = t < tiles ? __ldcg(tile_total + t) : 0u;
+        uint32_t sum;
+        const uint32_t ex = block_scan(tv, &sum);
+        if (t < tiles)
+            tile_off[t] = carry + ex;
+        carry += sum;
     }
     if (threadIdx.x == 0)
-        ctl->msf_count = s_warp[32];
+        ctl->msf_count = carry;
 }
 
 __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *out)
@@ -971,7 +993,8 @@ __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *
             if (lane >= (uint32_t)d)
                 incl += y;
         }
-        uint64_t pos = (uint64_t)__ldcs(a.chunk_cnt + c) + (incl - k);
+        const uint32_t *tile_off = a.chunk_cnt + gather_chunks(a.m) + gather_tiles(a.m);
+        uint64_t pos = (uint64_t)__ldcs(a.chunk_cnt + c) + __ldcg(tile_off + c / 4096) + (incl - k);
         // four of the lane's records per step, their loads in flight together
         while (bits) {
             uint32_t id[4];
@@ -1316,7 +1339,7 @@ size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
     c.take<uint32_t>(n);
     c.take<uint32_t>(n);
     c.take<uint32_t>((m + 31) / 32 + 4);
-    c.take<uint32_t>(gather_chunks(m));
+    c.take<uint32_t>(gather_words(m));
     c.take<uint4>(wl_capacity(m, sm_count));
     c.take<uint4>(wl_capacity(m, sm_count));
     return c.off;
@@ -1338,7 +1361,7 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     plan->cand[0] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
-    plan->chunk_cnt = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(gather_chunks(m)));
+    plan->chunk_cnt = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(gather_words(m)));
     plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->wl[1] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
     plan->e0 = d_e0;
@@ -1365,7 +1388,8 @@ phem_status msf_gather(phem_context *ctx, MsfPlan &plan, phem_edge *d_out)
     const uint64_t chunks = gather_chunks(plan.m);
     {
         KernelScope k(ctx, kKGather);
-        gather_scan_kernel<<<1, 1024, 0, ctx->stream>>>(plan.chunk_cnt, chunks, ctx->ctl);
+        gather_scan_kernel<<<(unsigned)gather_tiles(plan.m), 1024, 0, ctx->stream>>>(plan.chunk_cnt,
+                                                                                  gather_tiles(plan.m), ctx->ctl);
     }
     const uint64_t blocks_needed = (chunks + kGatherWarps - 1) / kGatherWarps;
     const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks_needed, (uint64_t)ctx->gather_blocks));
