@@ -239,7 +239,8 @@ struct MsfPlan {
     uint32_t n;
     uint32_t *parent;        // n
     unsigned long long *best;// n
-    uint32_t *cand[2];       // n each
+    uint32_t *cand;          // n: the round's choosers (hook -> compress)
+    uint32_t *samples;       // 8192: the threshold select's sampled weights
     uint32_t *bitmap;        // ceil(m / 32)
     uint32_t *chunk_cnt;     // MSF edges per 1024 edge ids, then their offsets (gather)
     uint4 *wl[2];            // m each

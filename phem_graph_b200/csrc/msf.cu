@@ -55,7 +55,7 @@ struct RoundArgs {
     uint32_t n;
     uint32_t *parent;
     unsigned long long *best;  // per component: minimum key (w << 32 | id) offered this round
-    uint32_t *cand0, *cand1;
+    uint32_t *cand0;  // the round's choosers
     uint32_t *bitmap;
     uint32_t *chunk_cnt;  // MSF edges per 1024 edge ids, then per-4096-chunk totals and offsets
     uint4 *wl0, *wl1;
@@ -184,7 +184,9 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 
 // ---- kernels -----------------------------------------------------------------
 
-__global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a, unsigned long long threshold)
+// set_threshold: 0 when the threshold select runs beside this kernel (it
+// writes ctl->threshold itself; both follow the control block's reset).
+__global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a, unsigned long long threshold, int set_threshold)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.n; x += stride) {
@@ -200,43 +202,75 @@ __global__ void __launch_bounds__(kBlock) init_kernel(RoundArgs a, unsigned long
         c->phase = 0;
         c->src = kSrcLight;
         c->cand_all = 1;
-        c->threshold = threshold;
+        if (set_threshold)
+            c->threshold = threshold;
     }
 }
 
 // Weight threshold from a stratified sample of kSample input weights: the
 // sample's `rank`-th smallest weight, found by a three-digit radix select in
-// shared memory (one CTA).  Light edges are those with w below it.
+// shared memory (by the last of the sampling CTAs).  Light edges are those
+// with w below it.
 constexpr int kSample = 8192;
 constexpr int kSelectThreads = 1024;
+constexpr int kSelectBlocks = kSample / kSelectThreads;
 
 __global__ void __launch_bounds__(kSelectThreads) select_threshold_kernel(const uint32_t *e0, uint64_t m,
-                                                                          uint64_t k, Ctl *ctl)
+                                                                          uint64_t k, uint32_t *g_samp, Ctl *ctl)
 {
     __shared__ uint32_t samp[kSample];
     __shared__ uint32_t hist[2048];
-    __shared__ uint32_t s_prefix, s_rank;
+    __shared__ uint32_t s_prefix, s_rank, s_or;
+    __shared__ bool s_last;
     const int tid = threadIdx.x;
-    // all of a thread's sample loads in flight together
+    // One sample per thread over kSelectBlocks blocks (a single block's 8192
+    // random reads queue behind one SM's outstanding-miss limit); the last
+    // block to finish selects.
+    {
+        const int i = blockIdx.x * kSelectThreads + tid;
+        const uint64_t lo = (uint64_t)i * m / kSample, hi = (uint64_t)(i + 1) * m / kSample;
+        const uint64_t pos = hi > lo ? lo + mix64(0x5EED0000ull + i) % (hi - lo) : lo;
+        g_samp[i] = __ldg(e0 + pos * 3 + 2);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ctl->misc[7], 1ull) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last)
+        return;
+    __threadfence();
+    if (tid == 0)
+        ctl->misc[7] = 0;
     constexpr int kPerThread = kSample / kSelectThreads;
     uint32_t v[kPerThread];
 #pragma unroll
-    for (int q = 0; q < kPerThread; q++) {
-        const int i = tid + q * kSelectThreads;
-        const uint64_t lo = (uint64_t)i * m / kSample, hi = (uint64_t)(i + 1) * m / kSample;
-        const uint64_t pos = hi > lo ? lo + mix64(0x5EED0000ull + i) % (hi - lo) : lo;
-        v[q] = __ldg(e0 + pos * 3 + 2);
-    }
-#pragma unroll
     for (int q = 0; q < kPerThread; q++)
+        v[q] = __ldcg(g_samp + tid + q * kSelectThreads);
+    uint32_t orv = 0;
+#pragma unroll
+    for (int q = 0; q < kPerThread; q++) {
         samp[tid + q * kSelectThreads] = v[q];
+        orv |= v[q];
+    }
     if (tid == 0) {
         s_prefix = 0;
         s_rank = (uint32_t)(k * kSample / m);
+        s_or = 0;
     }
+    __syncthreads();
+    orv = __reduce_or_sync(0xffffffffu, orv);
+    if ((tid & 31) == 0)
+        atomicOr(&s_or, orv);
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         const int sh = d == 0 ? 21 : (d == 1 ? 10 : 0), nb = d == 2 ? 10 : 11, hsh = sh + nb;
+        __syncthreads();
+        // a digit that is zero in every sample (weights below 2^21 leave the
+        // top one empty) puts them all in bin 0: the prefix and rank stand
+        if ((s_or >> sh) == 0)
+            continue;
         for (int i = tid; i < 2048; i += kSelectThreads)
             hist[i] = 0;
         __syncthreads();
@@ -687,6 +721,7 @@ __global__ void __launch_bounds__(kEpThreads, kEpMaxCtasPerSm) edge_pass_kernel(
 // flushes once more than 256 are pending (an iteration adds at most 256),
 // with one atomicAdd per flush and no barrier between warps.
 constexpr uint32_t kHookBuf = 512;
+constexpr int kHookCtasPerSm = 4;
 
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
@@ -777,6 +812,9 @@ __global__ void __launch_bounds__(kBlock) hook_kernel(RoundArgs a)
         flush();
 }
 
+// compress grid: four CTAs per SM, enough walks in flight for the
+// all-vertex rounds and a short launch for the late rounds' few choosers
+constexpr int kCompressCtasPerSm = 4;
 constexpr int kVItems = 4;  // candidates per thread per iteration of the vertex kernels
 
 // Pointer jumping over this round's choosers (the hook's list): each is
@@ -982,6 +1020,7 @@ __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *
     const uint64_t GW = (uint64_t)gridDim.x * kGatherWarps;
     const uint32_t *E = reinterpret_cast<const uint32_t *>(a.e0);
     unsigned long long wsum = 0;
+    const uint32_t *tile_off = a.chunk_cnt + gather_chunks(a.m) + gather_tiles(a.m);
     for (uint64_t c = gw; c < chunks; c += GW) {
         const uint64_t wd = c * 32 + lane;
         uint32_t bits = wd < words ? __ldcs(a.bitmap + wd) : 0u;
@@ -993,7 +1032,6 @@ __global__ void __launch_bounds__(kBlock) gather_kernel(RoundArgs a, phem_edge *
             if (lane >= (uint32_t)d)
                 incl += y;
         }
-        const uint32_t *tile_off = a.chunk_cnt + gather_chunks(a.m) + gather_tiles(a.m);
         uint64_t pos = (uint64_t)__ldcs(a.chunk_cnt + c) + __ldcg(tile_off + c / 4096) + (incl - k);
         // four of the lane's records per step, their loads in flight together
         while (bits) {
@@ -1041,8 +1079,7 @@ RoundArgs make_args(phem_context *ctx, const MsfPlan &p)
     a.n = p.n;
     a.parent = p.parent;
     a.best = p.best;
-    a.cand0 = p.cand[0];
-    a.cand1 = p.cand[1];
+    a.cand0 = p.cand;
     a.bitmap = p.bitmap;
     a.chunk_cnt = p.chunk_cnt;
     a.wl0 = p.wl[0];
@@ -1071,13 +1108,11 @@ phem_status queue_round(phem_context *ctx, const RoundArgs &a)
     }
     {
         KernelScope k(ctx, kKHook);
-        hook_kernel<KIND><<<ctx->sm_count * 4, kBlock, 0, ctx->stream>>>(a);
+        hook_kernel<KIND><<<ctx->sm_count * kHookCtasPerSm, kBlock, 0, ctx->stream>>>(a);
     }
     {
         KernelScope k(ctx, kKCompress);
-        // four CTAs per SM: enough walks in flight for the all-vertex rounds,
-        // and a short launch for the late rounds' few candidates
-        compress_kernel<<<std::min(vb, ctx->sm_count * 4), kBlock, 0, ctx->stream>>>(a, 0, 0);
+        compress_kernel<<<std::min(vb, ctx->sm_count * kCompressCtasPerSm), kBlock, 0, ctx->stream>>>(a, 0, 0);
     }
     PHEM_CUDA_TRY(cudaGetLastError());
     return PHEM_OK;
@@ -1145,30 +1180,31 @@ phem_status build_graph(phem_context *ctx, const MsfPlan &plan, const GraphKey &
         cudaGraph_t g;
         ~Drop() { cudaGraphDestroy(g); }
     } drop{g};
-    cudaGraphNode_t last, nn;
+    // Before the round loop, as a DAG: the control block's reset, then the
+    // vertex init and the threshold select side by side; the bitmap and
+    // chunk-count resets run beside all of them.
+    cudaGraphNode_t pre[4], n_ctl;
+    int npre = 0;
     RoundArgs a = key.a;
     unsigned long long thr = key.thr;
-    PHEM_TRY(add_memset(&last, g, nullptr, ctx->ctl, sizeof(Ctl)));
+    int set_thr = key.select ? 0 : 1;
+    PHEM_TRY(add_memset(&n_ctl, g, nullptr, ctx->ctl, sizeof(Ctl)));
     const size_t bitmap_bytes = ((plan.m + 31) / 32) * sizeof(uint32_t);
-    if (bitmap_bytes) {  // a memset node of zero bytes is invalid
-        PHEM_TRY(add_memset(&nn, g, &last, plan.bitmap, bitmap_bytes));
-        last = nn;
-    }
-    PHEM_TRY(add_memset(&nn, g, &last, plan.chunk_cnt, gather_chunks(plan.m) * sizeof(uint32_t)));
-    last = nn;
+    if (bitmap_bytes)  // a memset node of zero bytes is invalid
+        PHEM_TRY(add_memset(&pre[npre++], g, nullptr, plan.bitmap, bitmap_bytes));
+    PHEM_TRY(add_memset(&pre[npre++], g, nullptr, plan.chunk_cnt, gather_chunks(plan.m) * sizeof(uint32_t)));
     {
-        void *args[] = {&a, &thr};
-        PHEM_TRY(add_kernel(&nn, g, &last, init_kernel, dim3(key.vb_init), dim3(kBlock), args));
+        void *args[] = {&a, &thr, &set_thr};
+        PHEM_TRY(add_kernel(&pre[npre++], g, &n_ctl, init_kernel, dim3(key.vb_init), dim3(kBlock), args));
     }
-    last = nn;
     const uint32_t *e0w = static_cast<const uint32_t *>(plan.e0);
     uint64_t m = plan.m, k = key.k;
     Ctl *ctl = ctx->ctl;
     if (key.select) {
-        void *args[] = {&e0w, &m, &k, &ctl};
-        cudaGraphNode_t ns;
-        PHEM_TRY(add_kernel(&ns, g, &last, select_threshold_kernel, dim3(1), dim3(kSelectThreads), args));
-        last = ns;
+        uint32_t *samp = plan.samples;
+        void *args[] = {&e0w, &m, &k, &samp, &ctl};
+        PHEM_TRY(add_kernel(&pre[npre++], g, &n_ctl, select_threshold_kernel, dim3(kSelectBlocks),
+                            dim3(kSelectThreads), args));
     }
     cudaGraphConditionalHandle loop;
     PHEM_CUDA_TRY(cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault));
@@ -1178,7 +1214,7 @@ phem_status build_graph(phem_context *ctx, const MsfPlan &plan, const GraphKey &
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t nc;
-    PHEM_CUDA_TRY(cudaGraphAddNode(&nc, g, &last, 1, &cp));
+    PHEM_CUDA_TRY(cudaGraphAddNode(&nc, g, pre, npre, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     cudaGraphNode_t b0, b1, b2;
     {
@@ -1236,8 +1272,8 @@ phem_status run_impl(phem_context *ctx, MsfPlan &plan, uint32_t *rounds_out, boo
         key.select = filter && KIND == kKindMsf;
         key.ep_blocks = ctx->edge_pass_blocks;
         key.vb_init = vertex_blocks(ctx, plan.n);
-        key.vb_comp = std::min(vertex_blocks(ctx, plan.n), ctx->sm_count * 4);
-        key.hook_blocks = ctx->sm_count * 4;
+        key.vb_comp = std::min(vertex_blocks(ctx, plan.n), ctx->sm_count * kCompressCtasPerSm);
+        key.hook_blocks = ctx->sm_count * kHookCtasPerSm;
         key.kind = KIND;
         const bool cached = ctx->msf_exec[KIND] && std::memcmp(ctx->msf_key[KIND], &key, sizeof(key)) == 0;
         // a graph is built only for a solve seen twice in a row (same
@@ -1272,12 +1308,12 @@ stream_form:
     PHEM_CUDA_TRY(cudaMemsetAsync(plan.chunk_cnt, 0, gather_chunks(plan.m) * sizeof(uint32_t), s));
     {
         KernelScope ks(ctx, kKInit);
-        init_kernel<<<vertex_blocks(ctx, plan.n), kBlock, 0, s>>>(a, thr);
+        init_kernel<<<vertex_blocks(ctx, plan.n), kBlock, 0, s>>>(a, thr, 1);
     }
     if (filter && KIND == kKindMsf) {
         KernelScope ks(ctx, kKSelect);
-        select_threshold_kernel<<<1, kSelectThreads, 0, s>>>(static_cast<const uint32_t *>(plan.e0), plan.m, k,
-                                                             ctx->ctl);
+        select_threshold_kernel<<<kSelectBlocks, kSelectThreads, 0, s>>>(static_cast<const uint32_t *>(plan.e0),
+                                                                         plan.m, k, plan.samples, ctx->ctl);
     }
     PHEM_CUDA_TRY(cudaGetLastError());
     // Rounds are queued in batches; the host reads the continue flag between
@@ -1337,7 +1373,7 @@ size_t msf_workspace_bytes(uint64_t m, uint32_t n, int sm_count)
     c.take<uint32_t>(n);
     c.take<unsigned long long>(n);
     c.take<uint32_t>(n);
-    c.take<uint32_t>(n);
+    c.take<uint32_t>(kSample);
     c.take<uint32_t>((m + 31) / 32 + 4);
     c.take<uint32_t>(gather_words(m));
     c.take<uint4>(wl_capacity(m, sm_count));
@@ -1358,8 +1394,8 @@ phem_status msf_plan(phem_context *ctx, int kind, const void *d_e0, uint64_t m, 
     plan->status = ctx->status;
     plan->parent = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
     plan->best = reinterpret_cast<unsigned long long *>(base + k.take<unsigned long long>(n));
-    plan->cand[0] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
-    plan->cand[1] = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
+    plan->cand = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(n));
+    plan->samples = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(kSample));
     plan->bitmap = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>((m + 31) / 32 + 4));
     plan->chunk_cnt = reinterpret_cast<uint32_t *>(base + k.take<uint32_t>(gather_words(m)));
     plan->wl[0] = reinterpret_cast<uint4 *>(base + k.take<uint4>(wl_capacity(m, ctx->sm_count)));
