@@ -122,7 +122,7 @@ phem_status phem_context_launch_log(phem_context *ctx, phem_launch_record *out, 
  *                           queued on the stream in batches (per-launch
  *                           profiling always uses the stream form)        [1]
  *   "cc.canonical_light_per_vertex"  msf.light_per_vertex for the
- *                           PHEM_CC_CANONICAL forest (light = first by index) [2]
+ *                           PHEM_CC_CANONICAL forest (light = first by index) [1.5]
  *   "cc.sample_per_vertex"  phem_cc_solve unites this many edges per vertex
  *                           (a prefix of the list), compresses, then the
  *                           rest; 0 unites all at once                     [1]

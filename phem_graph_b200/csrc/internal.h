@@ -55,7 +55,7 @@ struct phem_context {
     bool msf_graph_select = false;       // ... and it had a threshold select
     // tuning knobs (phem_context_set_tuning)
     double tune_light_per_vertex = 0.5;  // light edges per vertex in the MSF filter (0: no filter)
-    double tune_canonical_light = 2.0;   // the same for the canonical CC forest (edges by index)
+    double tune_canonical_light = 1.5;   // the same for the canonical CC forest (edges by index)
     double tune_filter_min_ratio = 2.0;  // filter only when m >= ratio * light edges
     int tune_first_batch = 12;           // Boruvka rounds queued before the first host check
     int tune_next_batch = 4;             // rounds queued per later check
