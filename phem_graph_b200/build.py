@@ -34,7 +34,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-I", str(ROOT / "include
 CU_SOURCES = ["api.cu", "cc.cu", "msf.cu", "csr.cu", "noalloc.cu", "batch.cu", "batch_api.cu", "server.cu",
               "gen_dev.cu"]
 CXX_SOURCES = ["gen.cpp", "io.cpp"]
-HEADERS = ["common.cuh", "internal.h", "batch.h"]
+HEADERS = ["common.cuh", "internal.h", "batch.h", "uf.cuh"]
 
 
 def nvcc() -> str:

@@ -1,7 +1,8 @@
 // noalloc.cu -- connected components + spanning forest without allocating.
 //
-// phem_cc_solve_noalloc runs a one-pass union-find with phem_cc_solve's hook
-// rule, so its labels and forest mean the same (the reference's
+// phem_cc_solve_noalloc runs phem_cc_solve's union-find (the same union
+// steps, uf.cuh, and the same prefix / compress / rest schedule), so its
+// labels and forest mean the same (the reference's
 // init_parent_label_T1edges + union_find_gpu_COO + cc,
 // CC/ExternalSpanningTree.cu:77-116, CC/GPUSpanningTree.cu:122-128), with its
 // parent array in a fixed-size file-scope device array instead of a context
@@ -34,6 +35,7 @@
 #include <cuda_runtime.h>
 
 #include "internal.h"
+#include "uf.cuh"
 
 namespace phem {
 namespace {
@@ -45,55 +47,6 @@ static_assert(kNoallocMaxVertices == (1 << 20), "scratch size is part of the doc
 // The scratch: union-find parents and one status word (error bits).
 static __device__ __align__(256) int32_t g_noalloc_parent[kNoallocMaxVertices];
 static __device__ __align__(256) uint32_t g_noalloc_status;
-
-// Root of x with path halving over L2-coherent loads; bounded by n + 1 steps
-// (a path has at most n vertices), after which kErrChase is set.
-__device__ __forceinline__ int32_t na_find(int32_t *parent, int32_t x, int32_t n, uint32_t *status)
-{
-    for (uint32_t steps = 0; steps <= (uint32_t)n; steps++) {
-        const int32_t p = __ldcg(parent + x);
-        if (p == x)
-            return x;
-        const int32_t gp = __ldcg(parent + p);
-        if (gp == p)
-            return p;
-        parent[x] = gp;  // only non-roots are written, so no hook CAS is raced
-        x = gp;
-    }
-    set_err(status, kErrChase);
-    return x;
-}
-
-// The reference's union: edges with u < v only, larger root hooked under the
-// smaller by CAS, forest slot of the hooked root = the edge.
-__device__ __forceinline__ void na_unite(int32_t *parent, unsigned long long *forest, unsigned long long e,
-                                         int32_t n, uint32_t *status)
-{
-    int32_t u = (int32_t)(e >> 32), v = (int32_t)(uint32_t)e;
-    if (!(u < v))
-        return;
-    if (u < 0 || v >= n) {
-        set_err(status, kErrRange);
-        return;
-    }
-    for (uint32_t retry = 0; retry < kUnionRetryCap; retry++) {
-        const int32_t ru = na_find(parent, u, n, status);
-        const int32_t rv = na_find(parent, v, n, status);
-        if (ru == rv)
-            return;
-        if ((retry & 63) == 63 && (*(volatile uint32_t *)status & (kErrChase | kErrRetry)))
-            return;
-        const int32_t hi = ru > rv ? ru : rv, lo = ru > rv ? rv : ru;
-        if (atomicCAS(parent + hi, hi, lo) == hi) {
-            if (forest)
-                forest[hi] = e;
-            return;
-        }
-        u = ru;
-        v = rv;
-    }
-    set_err(status, kErrRetry);
-}
 
 __global__ void __launch_bounds__(kBlock) na_init_kernel(int32_t n, int32_t *parent, unsigned long long *forest,
                                                          uint32_t *status)
@@ -108,7 +61,8 @@ __global__ void __launch_bounds__(kBlock) na_init_kernel(int32_t n, int32_t *par
     }
 }
 
-// Two packed edges per 128-bit streaming load; the odd last edge alone.
+// Two packed edges per 128-bit streaming load (edges 16-byte aligned), the
+// odd last edge alone; the union is phem_cc_solve's (uf.cuh).
 __global__ void __launch_bounds__(kBlock) na_unite_kernel(const unsigned long long *edges, int64_t m, int32_t n,
                                                           int32_t *parent, unsigned long long *forest,
                                                           uint32_t *status)
@@ -118,11 +72,23 @@ __global__ void __launch_bounds__(kBlock) na_unite_kernel(const unsigned long lo
     const uint4 *q = reinterpret_cast<const uint4 *>(edges);
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < pairs; g += stride) {
         const uint4 a = __ldcs(q + g);
-        na_unite(parent, forest, ((unsigned long long)a.y << 32) | a.x, n, status);
-        na_unite(parent, forest, ((unsigned long long)a.w << 32) | a.z, n, status);
+        unite_packed(parent, forest, ((unsigned long long)a.y << 32) | a.x, n, status);
+        unite_packed(parent, forest, ((unsigned long long)a.w << 32) | a.z, n, status);
     }
     if ((m & 1) && blockIdx.x == 0 && threadIdx.x == 0)
-        na_unite(parent, forest, __ldcs(edges + m - 1), n, status);
+        unite_packed(parent, forest, __ldcs(edges + m - 1), n, status);
+}
+
+// Every vertex pointed at its root, so the next unions settle most edges
+// with two loads.
+__global__ void __launch_bounds__(kBlock) na_compress_kernel(int32_t n, int32_t *parent, uint32_t *status)
+{
+    const int32_t stride = gridDim.x * blockDim.x;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int32_t r = uf_find<true>(parent, i, n, status);
+        if (parent[i] != r)
+            parent[i] = r;
+    }
 }
 
 // label[i] = root(i), which is the smallest id of i's component.
@@ -130,10 +96,8 @@ __global__ void __launch_bounds__(kBlock) na_label_kernel(int32_t n, int32_t *pa
                                                           uint32_t *status)
 {
     const int32_t stride = gridDim.x * blockDim.x;
-    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const int32_t r = na_find(parent, i, n, status);
-        label[i] = r;
-    }
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        label[i] = uf_find<false>(parent, i, n, status);
 }
 
 struct NoallocScratch {
@@ -204,9 +168,19 @@ extern "C" phem_status phem_cc_solve_noalloc(const uint64_t *d_edges, int64_t m,
 
     na_init_kernel<<<na_grid(sm_count, n), kBlock, 0, st>>>(n, s.parent, forest, s.status);
     PHEM_CUDA_TRY(cudaGetLastError());
-    if (m > 0) {
-        na_unite_kernel<<<na_grid(sm_count, (m + 1) / 2), kBlock, 0, st>>>(
-            reinterpret_cast<const unsigned long long *>(d_edges), m, n, s.parent, forest, s.status);
+    // phem_cc_solve's schedule: a prefix of about one edge per vertex builds
+    // the big components, a compress points every vertex at its root, then
+    // the rest of the edges (an even prefix keeps the rest 16-byte aligned)
+    const unsigned long long *e = reinterpret_cast<const unsigned long long *>(d_edges);
+    const int64_t pre = m > n ? (int64_t)n & ~int64_t(1) : m;
+    if (pre > 0) {
+        na_unite_kernel<<<na_grid(sm_count, (pre + 1) / 2), kBlock, 0, st>>>(e, pre, n, s.parent, forest, s.status);
+        PHEM_CUDA_TRY(cudaGetLastError());
+    }
+    if (pre < m) {
+        na_compress_kernel<<<na_grid(sm_count, n), kBlock, 0, st>>>(n, s.parent, s.status);
+        na_unite_kernel<<<na_grid(sm_count, (m - pre + 1) / 2), kBlock, 0, st>>>(e + pre, m - pre, n, s.parent,
+                                                                                 forest, s.status);
         PHEM_CUDA_TRY(cudaGetLastError());
     }
     na_label_kernel<<<na_grid(sm_count, n), kBlock, 0, st>>>(n, s.parent, d_labels, s.status);
