@@ -244,8 +244,8 @@ phem_status phem_cc_merge(phem_context *ctx, const uint64_t *d_forest_a, const u
  * Runs on the current device and returns when the work is complete.
  * n > PHEM_CC_NOALLOC_MAX_VERTICES returns PHEM_ERR_INVALID.  Every call looks
  * the scratch address up in the current CUDA context (no allocation); the first
- * call on a device also loads the library's module there, so make it before any
- * stream capture.  All calls on a device share the scratch: calls that overlap
+ * call on a device also loads the library's module there.  All calls on a
+ * device share the scratch: calls that overlap
  * in time race and corrupt each other's results. */
 phem_status phem_cc_solve_noalloc(const uint64_t *d_edges, int64_t m, int32_t n, int32_t *d_labels,
                                   uint64_t *d_forest, void *stream);

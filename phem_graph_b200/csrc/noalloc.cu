@@ -25,8 +25,7 @@
 //     (cudaGetSymbolAddress: a table lookup, no allocation), so an address is
 //     never carried over from an earlier CUDA context of that device (after a
 //     cudaDeviceReset, or under a different driver context).  The first call
-//     on a device also loads this file's module: make that first call before
-//     any stream capture.
+//     on a device also loads this file's module.
 //   * Every call on one device uses the same scratch.  Calls that overlap in
 //     time (two host threads, or two streams with work in flight at once)
 //     race on it and corrupt each other's results; serialise them.
