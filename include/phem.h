@@ -217,6 +217,26 @@ phem_status phem_cc_stream(phem_context *ctx, const uint64_t *h_edges, int64_t m
                            int64_t batch, int32_t *d_parent, int32_t *d_label, uint64_t *d_forest,
                            float *ms);
 
+/* The same stream, one batch per call, for batches that arrive over time (a
+ * producer that reads or receives edges while earlier batches unite).
+ *   begin: initialises d_parent and d_forest (n entries, device; d_forest may be
+ *          NULL) and d_label (may be NULL) as phem_cc_stream does.
+ *   push:  unites edges[0..m) into the state.  A host batch (pinned for the
+ *          copy to overlap) is copied into one of two staging buffers of the
+ *          context while the previous batch's unions run; push returns when
+ *          the copy has landed, so the caller may refill its buffer at once.
+ *          A 16-byte aligned device batch is united in place and must stay
+ *          valid until the next push or end returns.
+ *   end:   waits for every union, reports a failed bound (status codes as
+ *          phem_cc_solve) and gives the time from begin to the last union.
+ * The state is then what phem_cc_stream leaves (phem_cc_label gives labels).
+ * One stream per context at a time; between begin and end the context runs
+ * no other solve (they would reset the status word the unions report into). */
+phem_status phem_cc_stream_begin(phem_context *ctx, int32_t n, int32_t *d_parent, int32_t *d_label,
+                                 uint64_t *d_forest);
+phem_status phem_cc_stream_push(phem_context *ctx, const uint64_t *edges, int64_t m);
+phem_status phem_cc_stream_end(phem_context *ctx, float *ms);
+
 /* Merge of two forests into final labels and a final forest.
  * gpu_spanning_tree (CC/GPUSpanningTree.cu:169-198): resets the state, unions
  * the 2n candidates d_forest_a[n] ++ d_forest_b[n] (PHEM_FOREST_EMPTY slots and

@@ -120,6 +120,9 @@ SIGNATURES = {
     "phem_cc_label": (C.c_int, [_VP, C.c_int32, _VP, _VP]),
     "phem_cc_stream": (C.c_int, [_VP, _VP, C.c_int64, C.c_int32, C.c_int64, _VP, _VP, _VP,
                                  C.POINTER(C.c_float)]),
+    "phem_cc_stream_begin": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
+    "phem_cc_stream_push": (C.c_int, [_VP, _VP, C.c_int64]),
+    "phem_cc_stream_end": (C.c_int, [_VP, C.POINTER(C.c_float)]),
     "phem_cc_merge": (C.c_int, [_VP, _VP, _VP, C.c_int32, _VP, _VP, _VP, C.POINTER(C.c_float)]),
     "phem_cc_solve_noalloc": (C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP, _VP]),
     "phem_msf_solve": (C.c_int, [_VP, _VP, C.c_uint64, C.c_uint32, _VP, C.POINTER(C.c_uint64),

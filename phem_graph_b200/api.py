@@ -244,6 +244,25 @@ class Context:
                                    C.byref(ms)), "phem_cc_stream")
         return ms.value
 
+    def cc_stream_begin(self, n: int, parent, label=None, forest=None):
+        """Opens an incremental stream (SpanningTree fed one batch per push)."""
+        check(lib().phem_cc_stream_begin(self._h, n, ptr(parent), ptr(label), ptr(forest)),
+              "phem_cc_stream_begin")
+
+    def cc_stream_push(self, edges):
+        """Unites one batch of packed edges (host or device); returns once a
+        host batch has been copied."""
+        m = len(edges) if isinstance(edges, np.ndarray) else int(edges.numel())
+        if isinstance(edges, np.ndarray):
+            edges = np.ascontiguousarray(edges, np.uint64)
+        check(lib().phem_cc_stream_push(self._h, ptr(edges), m), "phem_cc_stream_push")
+
+    def cc_stream_end(self) -> float:
+        """Waits for the stream's unions; the time from begin to the last one."""
+        ms = C.c_float()
+        check(lib().phem_cc_stream_end(self._h, C.byref(ms)), "phem_cc_stream_end")
+        return ms.value
+
     def cc_merge(self, forest_a, forest_b, n: int, parent, label, forest_out) -> float:
         """gpu_spanning_tree: merge two forests into final labels + forest."""
         ms = C.c_float()

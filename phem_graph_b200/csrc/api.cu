@@ -330,6 +330,20 @@ void phem_context_destroy(phem_context *ctx)
     for (auto e : ctx->event_pool)
         cudaEventDestroy(e);
     if (ctx->copy_stream)
+        cudaStreamSynchronize(ctx->copy_stream);
+    for (int b = 0; b < 2; b++) {
+        if (ctx->ccs.buf[b])
+            cudaFree(ctx->ccs.buf[b]);
+        if (ctx->ccs.copied[b])
+            cudaEventDestroy(ctx->ccs.copied[b]);
+        if (ctx->ccs.freed[b])
+            cudaEventDestroy(ctx->ccs.freed[b]);
+    }
+    if (ctx->ccs.t0)
+        cudaEventDestroy(ctx->ccs.t0);
+    if (ctx->ccs.t1)
+        cudaEventDestroy(ctx->ccs.t1);
+    if (ctx->copy_stream)
         cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream)
         cudaStreamDestroy(ctx->own_stream);
@@ -740,6 +754,134 @@ phem_status phem_cc_stream(phem_context *ctx, const uint64_t *h_edges, int64_t m
     PHEM_TRY(ctl_status(ctx->h_ctl->err, "cc_stream"));
     if (ms)
         *ms = t;
+    return PHEM_OK;
+}
+
+// Incremental SpanningTree: the batches of phem_cc_stream, handed over one
+// call at a time.  Host batches go through two staging buffers: batch k is
+// copied on the copy stream once the union that read its buffer (batch k - 2)
+// has finished, the union waits for its copy, and push returns when the copy
+// has landed, so the caller may refill its own buffer while the union runs.
+phem_status phem_cc_stream_begin(phem_context *ctx, int32_t n, int32_t *d_parent, int32_t *d_label,
+                                 uint64_t *d_forest)
+{
+    PHEM_TRY(check_ctx(ctx));
+    if (ctx->ccs.active) {
+        set_error("cc_stream_begin: a stream is already open on this context (end it first)");
+        return PHEM_ERR_INVALID;
+    }
+    if (n <= 0 || !d_parent || !is_device_ptr_on(d_parent, ctx->device) ||
+        (d_label && !is_device_ptr_on(d_label, ctx->device)) ||
+        (d_forest && !is_device_ptr_on(d_forest, ctx->device))) {
+        set_error("cc_stream_begin: need n > 0 and parent (label, forest) arrays in device memory of device %d",
+                  ctx->device);
+        return PHEM_ERR_INVALID;
+    }
+    DeviceGuard g(ctx->device);
+    auto &c = ctx->ccs;
+    for (int b = 0; b < 2; b++) {
+        if (!c.copied[b])
+            PHEM_CUDA_TRY(cudaEventCreateWithFlags(&c.copied[b], cudaEventDisableTiming));
+        if (!c.freed[b])
+            PHEM_CUDA_TRY(cudaEventCreateWithFlags(&c.freed[b], cudaEventDisableTiming));
+    }
+    if (!c.t0)
+        PHEM_CUDA_TRY(cudaEventCreate(&c.t0));
+    if (!c.t1)
+        PHEM_CUDA_TRY(cudaEventCreate(&c.t1));
+    PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), ctx->stream));
+    PHEM_TRY(cc_launch_init(ctx, n, d_parent, d_label, d_forest));
+    PHEM_CUDA_TRY(cudaEventRecord(c.t0, ctx->stream));
+    // both buffers free; the first copies wait for the init
+    for (int b = 0; b < 2; b++)
+        PHEM_CUDA_TRY(cudaEventRecord(c.freed[b], ctx->stream));
+    c.active = true;
+    c.n = n;
+    c.parent = d_parent;
+    c.forest = d_forest;
+    c.batches = c.edges = 0;
+    return PHEM_OK;
+}
+
+phem_status phem_cc_stream_push(phem_context *ctx, const uint64_t *edges, int64_t m)
+{
+    PHEM_TRY(check_ctx(ctx));
+    auto &c = ctx->ccs;
+    if (!c.active) {
+        set_error("cc_stream_push: no stream is open on this context (phem_cc_stream_begin)");
+        return PHEM_ERR_INVALID;
+    }
+    if (m < 0 || (m > 0 && !edges)) {
+        set_error("cc_stream_push: need m >= 0 and an edge array");
+        return PHEM_ERR_INVALID;
+    }
+    if (m == 0)
+        return PHEM_OK;
+    DeviceGuard g(ctx->device);
+    const bool dev = is_device_ptr(edges);
+    if (dev && !is_device_ptr_on(edges, ctx->device)) {
+        set_error("cc_stream_push: device edges must be memory of the context's device %d", ctx->device);
+        return PHEM_ERR_INVALID;
+    }
+    if (dev && ((uintptr_t)edges & 15) == 0) {
+        // a device batch is united in place (it stays valid until the next
+        // push or the end)
+        PHEM_TRY(cc_launch_unite(ctx, edges, m, c.n, c.parent, c.forest));
+    } else {
+        if ((size_t)m > c.cap) {
+            // grow both buffers once every copy and union that uses them is done
+            PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
+            PHEM_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            for (int b = 0; b < 2; b++) {
+                if (c.buf[b])
+                    cudaFree(c.buf[b]);
+                c.buf[b] = nullptr;
+            }
+            c.cap = 0;
+            const size_t cap = std::max<size_t>((size_t)m, 1u << 20);
+            for (int b = 0; b < 2; b++)
+                if (cudaMalloc(&c.buf[b], cap * sizeof(uint64_t)) != cudaSuccess) {
+                    cudaGetLastError();
+                    set_error("cc_stream_push: cannot allocate a %zu-edge staging buffer", cap);
+                    return PHEM_ERR_CUDA;
+                }
+            c.cap = cap;
+        }
+        const int b = (int)(c.batches & 1);
+        PHEM_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, c.freed[b], 0));
+        PHEM_CUDA_TRY(cudaMemcpyAsync(c.buf[b], edges, (size_t)m * sizeof(uint64_t), cudaMemcpyDefault,
+                                      ctx->copy_stream));
+        PHEM_CUDA_TRY(cudaEventRecord(c.copied[b], ctx->copy_stream));
+        PHEM_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, c.copied[b], 0));
+        PHEM_TRY(cc_launch_unite(ctx, c.buf[b], m, c.n, c.parent, c.forest));
+        PHEM_CUDA_TRY(cudaEventRecord(c.freed[b], ctx->stream));
+        // the caller's buffer is read once the copy has landed
+        PHEM_CUDA_TRY(cudaEventSynchronize(c.copied[b]));
+    }
+    c.batches++;
+    c.edges += m;
+    return PHEM_OK;
+}
+
+phem_status phem_cc_stream_end(phem_context *ctx, float *ms)
+{
+    PHEM_TRY(check_ctx(ctx));
+    auto &c = ctx->ccs;
+    if (!c.active) {
+        set_error("cc_stream_end: no stream is open on this context (phem_cc_stream_begin)");
+        return PHEM_ERR_INVALID;
+    }
+    c.active = false;
+    DeviceGuard g(ctx->device);
+    PHEM_CUDA_TRY(cudaEventRecord(c.t1, ctx->stream));
+    PHEM_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    PHEM_TRY(stream_wait(ctx));
+    PHEM_TRY(ctl_status(ctx->h_ctl->err, "cc_stream"));
+    if (ms) {
+        *ms = 0.f;
+        if (cudaEventElapsedTime(ms, c.t0, c.t1) != cudaSuccess)
+            *ms = 0.f;
+    }
     return PHEM_OK;
 }
 

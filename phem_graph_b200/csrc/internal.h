@@ -37,6 +37,19 @@ struct phem_context {
     void *input = nullptr;             // grow-only buffer for converted inputs (CSR -> records)
     size_t input_bytes = 0;
     uint64_t *status = nullptr;        // look-back status words, only ever written by look-back
+    // phem_cc_stream_begin/push/end: the stream in progress (the union-find
+    // state is the caller's) and two staging buffers of its own, so other
+    // solves between pushes may use the workspace
+    struct CcStream {
+        bool active = false;
+        int32_t n = 0;
+        int32_t *parent = nullptr;
+        uint64_t *forest = nullptr;
+        uint64_t *buf[2] = {nullptr, nullptr};
+        size_t cap = 0;                // edges per staging buffer
+        cudaEvent_t copied[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr}, t0 = nullptr, t1 = nullptr;
+        int64_t batches = 0, edges = 0;
+    } ccs;
     size_t status_words = 0;           // (zeroed when grown; epochs keep old words from matching)
     phem::Ctl *ctl = nullptr;          // device control block
     phem::Ctl *h_ctl = nullptr;        // pinned host mirror of the control block

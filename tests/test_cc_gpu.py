@@ -189,6 +189,68 @@ def test_stream_unsorted_rmat_batches(ctx):
     check_forest(pairs, n, got, forest.cpu().numpy().view(np.uint64))
 
 
+def test_incremental_stream_batches_of_every_kind(ctx):
+    """phem_cc_stream_begin/push/end: ragged batches from pinned and pageable
+    host memory (one larger than the first staging buffers, which then grow),
+    aligned device memory (united in place, one batch empty) and an unaligned
+    device view (staged): labels equal the oracle's and the forest reproduces
+    them."""
+    import torch
+    g = gen.er_graph(1 << 16, 1 << 21, 41)
+    n, pairs = g.n, g.pairs
+    cuts = [0, 1, 1001, 1001, 70001, 1270001, 1273000, len(pairs)]
+    dev = torch.device("cuda", ctx.device)
+    parent = torch.empty(n, dtype=torch.int32, device=dev)
+    label = torch.empty(n, dtype=torch.int32, device=dev)
+    forest = torch.empty(n, dtype=torch.int64, device=dev)
+    d_all = torch.from_numpy(pairs.view(np.int64)).to(dev)
+    ctx.cc_stream_begin(n, parent, label, forest)
+    for k in range(len(cuts) - 1):
+        a, b = cuts[k], cuts[k + 1]
+        kind = k % 4
+        if kind == 0:
+            ctx.cc_stream_push(torch.from_numpy(pairs[a:b].view(np.int64)).pin_memory())
+        elif kind == 1:
+            ctx.cc_stream_push(pairs[a:b].copy())
+        elif kind == 2:
+            ctx.cc_stream_push(d_all[a:b] if a % 2 == 0 else d_all[a:b].clone())
+        else:
+            ctx.cc_stream_push(d_all[a:b])  # odd start: 8-byte aligned only, staged
+    ms = ctx.cc_stream_end()
+    assert ms > 0
+    ctx.cc_label(n, parent, label)
+    torch.cuda.synchronize()
+    want, _ = oracle.cc_solve(pairs, n)
+    got = label.cpu().numpy()
+    np.testing.assert_array_equal(got, want)
+    check_forest(pairs, n, got, forest.cpu().numpy().view(np.uint64))
+
+
+def test_incremental_stream_call_order(ctx):
+    """push and end need an open stream; a second begin is refused; a stream
+    can be opened again after its end."""
+    import torch
+    n = 64
+    parent = torch.empty(n, dtype=torch.int32, device="cuda")
+    with pytest.raises(P.PhemError) as ei:
+        ctx.cc_stream_push(np.array([1], np.uint64))
+    assert ei.value.status == _lib.PHEM_ERR_INVALID
+    with pytest.raises(P.PhemError):
+        ctx.cc_stream_end()
+    ctx.cc_stream_begin(n, parent)
+    with pytest.raises(P.PhemError):
+        ctx.cc_stream_begin(n, parent)
+    ctx.cc_stream_push(np.array([(1 << 32) | 2, (2 << 32) | 3], np.uint64))
+    ctx.cc_stream_end()
+    ctx.cc_stream_begin(n, parent)
+    ctx.cc_stream_push(np.array([(5 << 32) | 9], np.uint64))
+    ctx.cc_stream_end()
+    label = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx.cc_label(n, parent, label)
+    got = label.cpu().numpy()
+    assert got[9] == 5 and got[3] == 3 and got[2] == 2  # only the second stream's edge
+
+
 @pytest.mark.parametrize("light", [0.0, 0.5, 2.0, 6.0])
 def test_canonical_filter_setting_does_not_change_the_forest(ctx, light):
     """The canonical forest's light/heavy split (first edges by index) gives
