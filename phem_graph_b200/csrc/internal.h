@@ -38,8 +38,8 @@ struct phem_context {
     size_t input_bytes = 0;
     uint64_t *status = nullptr;        // look-back status words, only ever written by look-back
     // phem_cc_stream_begin/push/end: the stream in progress (the union-find
-    // state is the caller's) and two staging buffers of its own, so other
-    // solves between pushes may use the workspace
+    // state is the caller's) and two staging buffers of its own, outside the
+    // workspace
     struct CcStream {
         bool active = false;
         int32_t n = 0;
