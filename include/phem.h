@@ -316,7 +316,10 @@ phem_status phem_msf_stream(phem_context *ctx, const phem_edge *h_edges, uint64_
 /* MSF of a symmetrised CSR graph (int64 offsets[n + 1], uint32 cols[2m]).
  * Edge i is the i-th entry with row < col in row-major order (the numbering of
  * csr_to_coo, CC/graph.cu:169-187); weights[i] is its weight.  Output as
- * phem_msf_solve. */
+ * phem_msf_solve.  m_upper must be the number of such entries: the count is
+ * checked once the solve has run (no host round trip sits between the
+ * conversion and the solve), and a mismatch returns PHEM_ERR_INVALID with the
+ * outputs unspecified. */
 phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const uint32_t *cols,
                                uint32_t n, const uint32_t *weights, uint64_t m_upper,
                                phem_edge *msf, uint64_t *count, uint64_t *total,

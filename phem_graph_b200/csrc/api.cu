@@ -1200,21 +1200,31 @@ phem_status phem_msf_solve_csr(phem_context *ctx, const int64_t *offsets, const 
     phem_edge *d_rec = reinterpret_cast<phem_edge *>(b + o_rec);
     // one pass: kept entry p becomes the record {row, col, weights[p]}
     phem_status st = csr_launch_to_coo(ctx, d_off, d_col, (int32_t)n, nnz, d_tr, nullptr, d_w, d_rec, m_upper);
-    if (st == PHEM_OK && cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost,
+    // The solve is queued behind the conversion with no host round trip
+    // between them; the conversion's count of entries with row < col is kept
+    // aside (the solve resets the control block) and checked afterwards.  The
+    // conversion writes no record past m_upper, and a short count leaves stale
+    // records that the solve range-checks like any input, so a mismatch only
+    // discards the solve's result.
+    uint64_t *d_kept = reinterpret_cast<uint64_t *>(b + o_rec + align256(rb));
+    if (st == PHEM_OK && cudaMemcpyAsync(d_kept, &ctx->ctl->misc[2], sizeof(uint64_t), cudaMemcpyDeviceToDevice,
                                          ctx->stream) != cudaSuccess)
         st = PHEM_ERR_CUDA;
-    if (st == PHEM_OK)
-        st = stream_wait(ctx);
-    if (st == PHEM_OK)
-        st = ctl_status(ctx->h_ctl->err, "msf_solve_csr");
-    if (st == PHEM_OK && ctx->h_ctl->misc[2] != m_upper) {
+    if (st != PHEM_OK)
+        return st;
+    const phem_status solved = msf_common(ctx, d_rec, m_upper, n, msf, count, total, stats, nullptr);
+    uint64_t kept = 0;
+    if (cudaMemcpyAsync(&ctx->h_ctl->misc[2], d_kept, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream) !=
+        cudaSuccess)
+        return PHEM_ERR_CUDA;
+    PHEM_TRY(stream_wait(ctx));
+    kept = ctx->h_ctl->misc[2];
+    if (kept != m_upper) {
         set_error("msf_solve_csr: CSR has %llu entries with row < col, m_upper = %llu",
-                  (unsigned long long)ctx->h_ctl->misc[2], (unsigned long long)m_upper);
-        st = PHEM_ERR_INVALID;
+                  (unsigned long long)kept, (unsigned long long)m_upper);
+        return PHEM_ERR_INVALID;
     }
-    if (st == PHEM_OK)
-        st = msf_common(ctx, d_rec, m_upper, n, msf, count, total, stats, nullptr);
-    return st;
+    return solved;
 }
 
 phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, int32_t n,

@@ -4,7 +4,7 @@
 // for every entry with i < col.  Here the entries are cut into tiles of
 // kCsrTile consecutive entries on a static grid-stride schedule (no block
 // waits for another, so the loads of independent tiles overlap freely); a
-// tile is kCsrWarps segments of 512 entries, one per warp, read lane-striped
+// tile is kCsrWarps segments of 256 entries, one per warp, read lane-striped
 // (step k of lane L holds entry 32k + L of the segment, so every load and
 // store is one contiguous warp access):
 //   1. csr_tile_rows_kernel, one thread per row, writes for every tile the row
@@ -14,9 +14,12 @@
 //      the row each warp segment starts in; a warp then resolves the row of
 //      every entry with one ballot per step (the latest mark at or before the
 //      lane) and counts the entries with row < col;
-//   3. csr_scan_kernel (one block) turns the tile counts into tile offsets;
+//   3. csr_scan_kernel turns the tile counts into tile offsets: every block
+//      scans a group of 4096 tiles and the last block to finish scans the
+//      groups' totals (no block waits for another);
 //   4. csr_write_kernel resolves the rows again and writes the kept entries in
-//      order: tile offset + the warps before + the lanes before (ballot).
+//      order: group offset + tile offset + the warps before + the lanes before
+//      (ballot).
 // Every entry keeps its place in the reference's row walk, so the output order
 // (and therefore the edge numbering) is exactly the reference's.  The record
 // form fuses the MSF CSR input's packing: the kept entry at position p becomes
@@ -29,14 +32,15 @@
 namespace phem {
 namespace {
 
-constexpr int kCsrThreads = 128;                  // threads per block of passes 2 and 4
+constexpr int kCsrThreads = 256;                  // threads per block of passes 2 and 4
 constexpr int kCsrWarps = kCsrThreads / 32;
-constexpr int kCsrItems = 16;                     // entries per lane per tile
-constexpr int kCsrSeg = 32 * kCsrItems;           // 512 entries per warp segment
+constexpr int kCsrItems = 8;                      // entries per lane per tile
+constexpr int kCsrSeg = 32 * kCsrItems;           // 256 entries per warp segment
 constexpr int kCsrTile = kCsrWarps * kCsrSeg;     // 2048 entries per tile
-constexpr int kCsrBlocksPerSm = 6;                // resident blocks per SM (register bound)
+constexpr int kCsrBlocksPerSm = 6;                // resident blocks per SM: 48 warps (registers <= 42)
 constexpr int kScanBlock = 1024;
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 4;
+constexpr int kScanGroup = kScanBlock * kScanItems;  // tiles per block of pass 3
 
 // tile_rows[t] = the row i with offsets[i] <= t * kCsrTile < offsets[i + 1].
 // Malformed offsets leave tiles unwritten; the conversion clamps what it reads.
@@ -175,30 +179,29 @@ __global__ void __launch_bounds__(kCsrThreads, kCsrBlocksPerSm)
     }
 }
 
-// Pass 3 (one block): prefix[t] = kept entries before tile t; the total to *kept.
+// Pass 3: prefix[t] = kept entries before tile t within its group of
+// kScanGroup tiles (one block per group, kScanItems tiles per thread); the
+// last block to finish scans the group totals into group_off[] and writes
+// the whole count to *kept.
 __global__ void __launch_bounds__(kScanBlock) csr_scan_kernel(const uint32_t *counts, uint32_t ntiles,
-                                                              uint32_t *prefix, unsigned long long *kept)
+                                                              uint32_t *prefix, uint32_t *group_tot,
+                                                              uint32_t *group_off, unsigned long long *kept,
+                                                              unsigned long long *ticket)
 {
     __shared__ uint32_t s_w[kScanBlock / 32 + 1];
+    __shared__ bool s_last;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    uint64_t carry = 0;
-    for (uint64_t base = 0; base < ntiles; base += (uint64_t)kScanBlock * kScanItems) {
-        const uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
-        uint32_t v[kScanItems], sum = 0;
-#pragma unroll
-        for (int k = 0; k < kScanItems; k++) {
-            v[k] = i0 + k < ntiles ? counts[i0 + k] : 0u;
-            sum += v[k];
-        }
-        uint32_t x = sum;
+    // exclusive scan of one value per thread over the block; *total = the sum
+    auto block_scan = [&](uint32_t x, uint32_t *total) {
+        uint32_t inc = x;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
             if (lane >= (uint32_t)d)
-                x += y;
+                inc += y;
         }
         if (lane == 31)
-            s_w[warp] = x;
+            s_w[warp] = inc;
         __syncthreads();
         if (warp == 0) {
             const uint32_t a = s_w[lane];
@@ -214,15 +217,46 @@ __global__ void __launch_bounds__(kScanBlock) csr_scan_kernel(const uint32_t *co
                 s_w[32] = z;
         }
         __syncthreads();
-        uint32_t run = (uint32_t)carry + s_w[warp] + x - sum;
+        *total = s_w[32];
+        const uint32_t r = s_w[warp] + inc - x;
+        __syncthreads();  // s_w is reused
+        return r;
+    };
+    const uint64_t i0 = (uint64_t)blockIdx.x * kScanGroup + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], sum = 0;
 #pragma unroll
-        for (int k = 0; k < kScanItems; k++)
-            if (i0 + k < ntiles) {
-                prefix[i0 + k] = run;
-                run += v[k];
-            }
-        carry += s_w[32];
-        __syncthreads();
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = i0 + k < ntiles ? counts[i0 + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t total;
+    uint32_t run = block_scan(sum, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+        if (i0 + k < ntiles) {
+            prefix[i0 + k] = run;
+            run += v[k];
+        }
+    if (threadIdx.x == 0) {
+        group_tot[blockIdx.x] = total;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1ull) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last)
+        return;
+    __threadfence();
+    if (threadIdx.x == 0)
+        *ticket = 0;
+    uint64_t carry = 0;
+    for (uint32_t g0 = 0; g0 < gridDim.x; g0 += kScanBlock) {
+        const uint32_t g = g0 + threadIdx.x;
+        const uint32_t x = g < gridDim.x ? __ldcg(group_tot + g) : 0u;
+        uint32_t s;
+        const uint32_t ex = block_scan(x, &s);
+        if (g < gridDim.x)
+            group_off[g] = (uint32_t)carry + ex;
+        carry += s;
     }
     if (threadIdx.x == 0)
         *kept = carry;
@@ -233,8 +267,8 @@ __global__ void __launch_bounds__(kScanBlock) csr_scan_kernel(const uint32_t *co
 template <bool RECORDS>
 __global__ void __launch_bounds__(kCsrThreads, kCsrBlocksPerSm)
     csr_write_kernel(const int64_t *offsets, const uint32_t *cols, int32_t n, int64_t nnz,
-                     const uint32_t *tile_rows, const uint32_t *prefix, unsigned long long *out, const uint32_t *w,
-                     phem_edge *rec_out, uint64_t cap)
+                     const uint32_t *tile_rows, const uint32_t *prefix, const uint32_t *group_off,
+                     unsigned long long *out, const uint32_t *w, phem_edge *rec_out, uint64_t cap)
 {
     __shared__ uint32_t s_mark[kCsrTile];
     __shared__ uint32_t s_seg[kCsrWarps];
@@ -259,7 +293,7 @@ __global__ void __launch_bounds__(kCsrThreads, kCsrBlocksPerSm)
         for (int k = 0; k < kCsrItems; k++)
             col[k] = nc[k];
         const int32_t row0 = s_row[buf][0], row1 = s_row[buf][1];
-        const uint32_t base = __ldg(prefix + t);
+        const uint32_t base = __ldg(prefix + t) + __ldg(group_off + t / kScanGroup);
         const uint32_t tn = t + gridDim.x;
         if (threadIdx.x == 0)
             load_row_range(tile_rows, n, tn, ntiles, s_row[buf ^ 1]);
@@ -305,7 +339,8 @@ __global__ void __launch_bounds__(kCsrThreads, kCsrBlocksPerSm)
 size_t csr_scratch_bytes(int64_t nnz)
 {
     const size_t tiles = (size_t)((nnz + kCsrTile - 1) / kCsrTile);
-    return align256((3 * tiles + 1) * sizeof(uint32_t));
+    const size_t groups = (tiles + kScanGroup - 1) / kScanGroup;
+    return align256((3 * tiles + 1 + 2 * groups) * sizeof(uint32_t));
 }
 
 phem_status csr_launch_to_coo(phem_context *ctx, const int64_t *offsets, const uint32_t *cols, int32_t n,
@@ -321,7 +356,9 @@ phem_status csr_launch_to_coo(phem_context *ctx, const int64_t *offsets, const u
         PHEM_CUDA_TRY(cudaMemsetAsync(&ctx->ctl->misc[2], 0, sizeof(unsigned long long), ctx->stream));
         return PHEM_OK;
     }
+    const uint64_t groups = (tiles + kScanGroup - 1) / kScanGroup;
     uint32_t *tile_rows = scratch, *counts = scratch + tiles + 1, *prefix = counts + tiles;
+    uint32_t *group_tot = prefix + tiles, *group_off = group_tot + groups;
     const int blocks = (int)std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * kCsrBlocksPerSm);
     {
         KernelScope k(ctx, kKCsrCoo);
@@ -334,15 +371,18 @@ phem_status csr_launch_to_coo(phem_context *ctx, const int64_t *offsets, const u
         KernelScope k(ctx, kKCsrCoo);
         csr_count_kernel<<<blocks, kCsrThreads, 0, ctx->stream>>>(offsets, cols, n, nnz, tile_rows, counts);
     }
+    PHEM_CUDA_TRY(cudaMemsetAsync(&ctx->ctl->misc[3], 0, sizeof(unsigned long long), ctx->stream));  // scan ticket
     {
         KernelScope k(ctx, kKCsrCoo);
-        csr_scan_kernel<<<1, kScanBlock, 0, ctx->stream>>>(counts, (uint32_t)tiles, prefix, &ctx->ctl->misc[2]);
+        csr_scan_kernel<<<(unsigned)groups, kScanBlock, 0, ctx->stream>>>(counts, (uint32_t)tiles, prefix, group_tot,
+                                                                         group_off, &ctx->ctl->misc[2],
+                                                                         &ctx->ctl->misc[3]);
     }
     if (records || out) {
         KernelScope k(ctx, kKCsrCoo);
         auto *o = reinterpret_cast<unsigned long long *>(out);
         (records ? csr_write_kernel<true> : csr_write_kernel<false>)<<<blocks, kCsrThreads, 0, ctx->stream>>>(
-            offsets, cols, n, nnz, tile_rows, prefix, o, w, records, cap);
+            offsets, cols, n, nnz, tile_rows, prefix, group_off, o, w, records, cap);
     }
     PHEM_CUDA_TRY(cudaGetLastError());
     return PHEM_OK;

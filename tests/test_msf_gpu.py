@@ -234,6 +234,26 @@ def test_csr_shapes(ctx, kind):
     assert_msf(r, E, ids, cnt, tot)
 
 
+def test_csr_many_scan_groups_and_wrong_edge_count(ctx):
+    """A CSR of 16.8 M entries (8,192 tiles: two groups of the tile-offset
+    scan) converts in the reference's order and solves exactly; an edge count
+    that disagrees with the CSR is reported after the solve (too low or too
+    high), and the context solves correctly afterwards."""
+    g = gen.rmat_graph(19, 16, seed=19)
+    off, cols = gen.csr_from_pairs(g.pairs, g.n)
+    assert (len(cols) + 2047) // 2048 > 4096
+    np.testing.assert_array_equal(ctx.csr_to_coo(off, cols, g.n), oracle.csr_to_coo(off, cols, g.n))
+    E = g.msf_edges()
+    ids, cnt, tot = expect(E, g.n)
+    for bad in (g.m - 1, g.m + 5):
+        w = np.zeros(bad, np.uint32)
+        w[: min(bad, g.m)] = g.w[: min(bad, g.m)]
+        with pytest.raises(P.PhemError) as ei:
+            ctx.msf_solve_csr(off, cols, g.n, w, bad)
+        assert ei.value.status == _lib.PHEM_ERR_INVALID
+    assert_msf(ctx.msf_solve_csr(off, cols, g.n, g.w, g.m), E, ids, cnt, tot)
+
+
 def test_csr_device_buffers(ctx):
     """Device offsets/cols/output take the no-staging path."""
     import torch
