@@ -1253,6 +1253,8 @@ phem_status phem_csr_to_coo(phem_context *ctx, const int64_t *offsets, const uin
     PHEM_TRY(stage_in(ctx, offsets, ob, o_off, &so));
     PHEM_TRY(stage_in(ctx, cols, cb, o_col, &sc));
     stage_out(ctx, out, 0, o_out, &sx);
+    // a status bit an earlier call left set is not this call's
+    PHEM_CUDA_TRY(cudaMemsetAsync(ctx->ctl, 0, sizeof(Ctl), ctx->stream));
     // host output: stage only as much as can be kept (at most nnz / 2 entries have row < col
     // in a symmetric CSR; a non-symmetric one may keep more, so count first in that case)
     if (sx.host) {
